@@ -1,0 +1,190 @@
+/*
+ * lfm_b200.h -- C ABI of the B200 (sm_100a) leapfrog library liblfm_b200.so.
+ *
+ * One call advances one lattice by one leapfrog step of GOV-01 (Psi) and
+ * GOV-02 (chi) over the periodic 19-point Laplacian, with the cos^2 sponge,
+ * the chi >= -chi0 clamp and, at the COLOR level, the cross-colour, f_c,
+ * CCV and SCV terms.  All pointers are device pointers unless a parameter
+ * name ends in _host.  Arrays are flat float32 in C order,
+ * idx = (i*N + j)*N + k; colour arrays are [colour][i][j][k] with 3 colours.
+ * Every entry point returns 0 (LFM_OK) or an LFM_ERR_* code; lfm_strerror()
+ * names it and lfm_last_error_detail() gives the message of the calling
+ * thread's last failure.  Launches are asynchronous on `stream` (a
+ * cudaStream_t passed as void*; NULL = legacy default stream).
+ *
+ * Scalar parameters are the reference's Python floats (double).  They are
+ * rounded to float32 inside the library exactly as NumPy rounds a Python
+ * float meeting a float32 array, so the plain float32 steps reproduce the
+ * reference's NumPy float32 path bit for bit.
+ */
+#ifndef LFM_B200_H
+#define LFM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LFM_B200_ABI_VERSION 1
+
+enum lfm_status {
+  LFM_OK = 0,
+  LFM_ERR_INVALID_ARG = 1,   /* bad size, null pointer, overlapping buffers */
+  LFM_ERR_ALIGNMENT = 2,     /* a device pointer is not 16-byte aligned */
+  LFM_ERR_UNSUPPORTED = 3,   /* combination this build does not provide */
+  LFM_ERR_CUDA = 4,          /* a CUDA runtime call failed */
+  LFM_ERR_CUFFT = 5,         /* a cuFFT call failed */
+  LFM_ERR_MASK = 6,          /* mask is not a function of the radial key q */
+  LFM_ERR_DEVICE_TIMEOUT = 7,/* a bounded device-side wait gave up */
+  LFM_ERR_NONFINITE = 8,     /* a reduction met NaN/Inf */
+  LFM_ERR_CAPACITY = 9       /* output table or scratch too small */
+};
+
+/* Field levels, as lfm.config.FieldLevel (lfm/config.py:36-46). */
+enum lfm_level { LFM_REAL = 0, LFM_COMPLEX = 1, LFM_COLOR = 2 };
+
+const char* lfm_strerror(int status);
+const char* lfm_last_error_detail(void);
+int lfm_abi_version(void);
+
+/* ------------------------------------------------------------------------
+ * Sponge mask lookup table.
+ *
+ * The reference's mask (lfm/core/backends/numpy_backend.py:49-69) is a pure
+ * function of the integer key q = (2i-N+1)^2 + (2j-N+1)^2 + (2k-N+1)^2
+ * (4*R^2 in the reference's float32 coordinates, exact for N <= 2048).
+ * lfm_mask_lut_build scans the host copy of the N^3 mask and stores, for the
+ * band q_lo <= q <= q_hi where the mask is neither 0 nor 1, one float32 per
+ * key step of 2^shift.  The step kernels then read 4 bytes per cell from an
+ * L1-resident table instead of streaming the N^3 mask.  The values are the
+ * host mask's own float32 values, so the table is bit-exact.  Returns
+ * LFM_ERR_MASK if two cells with the same q hold different values.
+ * ------------------------------------------------------------------------ */
+typedef struct lfm_mask_lut {
+  int32_t N;      /* lattice edge */
+  int32_t shift;  /* table index = (q - q_lo) >> shift; 3 for even N, 2 for odd N */
+  int32_t q_lo;   /* q < q_lo: mask 0 */
+  int32_t q_hi;   /* q > q_hi: mask 1 */
+  int32_t count;  /* table entries used */
+} lfm_mask_lut;
+
+int lfm_mask_lut_build(int N, const float* mask_host, float* table_host, int capacity,
+                       lfm_mask_lut* out);
+
+/* ------------------------------------------------------------------------
+ * Protocol steps: the reference Backend's step_* calls, one for one.
+ *
+ * Replace lfm/core/backends/cupy_backend.py:127-169 (step_real),
+ * :171-222 (step_complex) and :224-317 (step_color), whose kernels are
+ * evolve_real / evolve_complex / evolve_gov01_gov02 in
+ * lfm/core/backends/kernel_source.py:323-419, :424-540, :18-235.  Inputs
+ * and outputs are separate buffers (the reference's A/B double buffer):
+ * psi_out = damped new field, psi_prev_out = damped current field,
+ * chi_out = new chi, chi_prev_out = current chi.  boundary_mask is the
+ * device copy of the N^3 mask.
+ * ------------------------------------------------------------------------ */
+int lfm_step_real_f32(const float* psi_in, const float* psi_prev_in, const float* chi_in,
+                      const float* chi_prev_in, const float* boundary_mask, float* psi_out,
+                      float* psi_prev_out, float* chi_out, float* chi_prev_out, int N,
+                      double dt2, double kappa, double lambda_self, double chi0,
+                      double e0_sq, void* stream);
+
+int lfm_step_complex_f32(const float* psi_r_in, const float* psi_r_prev_in,
+                         const float* psi_i_in, const float* psi_i_prev_in,
+                         const float* chi_in, const float* chi_prev_in,
+                         const float* boundary_mask, float* psi_r_out, float* psi_r_prev_out,
+                         float* psi_i_out, float* psi_i_prev_out, float* chi_out,
+                         float* chi_prev_out, int N, double dt2, double kappa,
+                         double lambda_self, double chi0, double e0_sq, double epsilon_w,
+                         void* stream);
+
+/* sa_fields_out (3*N^3, may be NULL) receives the clipped S_a fields when
+ * kappa_tube > 0, as numpy_backend.py:341-356; sa_fields_in is accepted for
+ * signature parity and, like the reference, not read when kappa_tube > 0.
+ * The S_a solve needs cuFFT plans and spectrum scratch, held in `ctx`
+ * (see lfm_context_create); ctx may be NULL when kappa_tube == 0. */
+typedef struct lfm_context lfm_context;
+
+int lfm_step_color_f32(lfm_context* ctx, const float* psi_r_in, const float* psi_r_prev_in,
+                       const float* psi_i_in, const float* psi_i_prev_in,
+                       const float* chi_in, const float* chi_prev_in,
+                       const float* boundary_mask, float* psi_r_out, float* psi_r_prev_out,
+                       float* psi_i_out, float* psi_i_prev_out, float* chi_out,
+                       float* chi_prev_out, int N, double dt2, double kappa,
+                       double lambda_self, double chi0, double e0_sq, double epsilon_w,
+                       double kappa_c, double epsilon_cc, double kappa_string,
+                       double kappa_tube, const float* sa_fields_in, float* sa_fields_out,
+                       double sa_gamma, double sa_d, double dt, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Library context: cuFFT plans and spectrum scratch for the S_a solve,
+ * keyed by lattice edge, on the device that is current at creation.
+ * Replaces the per-step plan/filter rebuild of cupy_backend.py:261-279.
+ * ------------------------------------------------------------------------ */
+int lfm_context_create(lfm_context** out);
+int lfm_context_destroy(lfm_context* ctx);
+
+/* ------------------------------------------------------------------------
+ * Resident-lattice steps (the fast path behind lfm_b200.Evolver).
+ *
+ * Same arithmetic as the protocol steps, but each field keeps two slots and
+ * the step writes the new values into the slot that held the previous ones:
+ * psi_prev_io is read at each cell and then overwritten with the new psi,
+ * chi_prev_io likewise with the new chi.  The caller then swaps the roles of
+ * the slots.  Because the reference stores psi_prev' = (1-mask)*psi, a slot
+ * that was written by the previous call holds the undamped field; pass
+ * damp_prev = 1 to apply (1-mask) on read (the same single float32 product,
+ * so the result is unchanged bit for bit), or 0 when the host wrote the
+ * previous field itself.  chi's previous field is never damped.
+ * The mask comes from the lookup table (table = device copy of the table
+ * built by lfm_mask_lut_build).  Moves 24 B/cell (REAL), 36 B (COMPLEX).
+ * ------------------------------------------------------------------------ */
+int lfm_leapfrog_real_f32(const float* psi, float* psi_prev_io, const float* chi,
+                          float* chi_prev_io, const float* mask_table,
+                          const lfm_mask_lut* lut, int damp_prev, int N, double dt2,
+                          double kappa, double lambda_self, double chi0, double e0_sq,
+                          void* stream);
+
+int lfm_leapfrog_complex_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                             float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                             const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                             int N, double dt2, double kappa, double lambda_self,
+                             double chi0, double e0_sq, double epsilon_w, void* stream);
+
+/* sa: raw (unclipped) S_a fields from lfm_helmholtz_sa_f32 of this step's
+ * psi, or NULL when kappa_tube == 0; the kernel clips them at 0 on read. */
+int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                           float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                           const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                           int N, double dt2, double kappa, double lambda_self, double chi0,
+                           double e0_sq, double epsilon_w, double kappa_c, double epsilon_cc,
+                           double kappa_string, double kappa_tube, const float* sa,
+                           void* stream);
+
+/* ------------------------------------------------------------------------
+ * S_a Helmholtz solve (numpy_backend.py:341-356, cupy_backend.py:261-279):
+ * sa_raw[a] = IRFFT[ gamma/(gamma + D|k|^2) * RFFT(|Psi_a|^2) ] for a = 0..2,
+ * k = 2*pi*fftfreq(N), computed in float32 with cuFFT (R2C, hand-written
+ * k-space multiply with 1/N^3 folded in, C2R).  sa_raw is NOT clipped;
+ * consumers clip at 0 (lfm_sa_clip_f32 for a host-visible copy).
+ * ------------------------------------------------------------------------ */
+int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
+                         float* sa_raw, int N, double sa_gamma, double sa_d, void* stream);
+int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* stream);
+
+/* Kernel path for the step calls: 0 = automatic (fused 2.5D kernel where
+ * it applies, the direct kernel otherwise), 1 = direct kernel only,
+ * 2 = fused kernel only (calls it cannot serve return LFM_ERR_UNSUPPORTED).
+ * Process-wide; for tests and tuning. */
+int lfm_set_step_path(int path);
+
+/* Reads (and optionally clears) the device status word that bounded
+ * device-side waits set on timeout; synchronises the current device. */
+int lfm_device_status(int* status_out, int clear);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LFM_B200_H */

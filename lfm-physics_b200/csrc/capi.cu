@@ -1,0 +1,544 @@
+// C ABI of liblfm_b200.so (declared in include/lfm_b200.h): argument
+// checks, kernel-path choice, the sponge lookup table, and the library
+// context that owns the cuFFT plans and scratch of the S_a solve.
+#include <cufft.h>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "lfm_b200.h"
+#include "lfm_kernels.h"
+
+// Device status word: bounded device-side waits OR an LFM_ERR_* code into
+// it when they give up (read back with lfm_device_status).
+__device__ int g_lfm_status;
+
+namespace {
+
+thread_local std::string t_detail;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  t_detail = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(LFM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Kernel path: 0 = choose (fused 2.5D kernel when it applies), 1 = direct
+// kernel only, 2 = fused kernel only (LFM_ERR_UNSUPPORTED when it cannot run).
+std::atomic<int> g_path{0};
+
+constexpr int kMaxDevices = 64;
+std::mutex g_status_mu;
+int* g_status_ptr[kMaxDevices] = {nullptr};
+
+int status_word(int** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(LFM_ERR_UNSUPPORTED, "device %d", dev);
+  std::lock_guard<std::mutex> lk(g_status_mu);
+  if (!g_status_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_lfm_status);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_lfm_status)");
+    g_status_ptr[dev] = static_cast<int*>(p);
+  }
+  *out = g_status_ptr[dev];
+  return LFM_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int check_n(int N) {
+  if (N < 2 || N > 2048) return fail(LFM_ERR_INVALID_ARG, "N=%d outside [2, 2048]", N);
+  return LFM_OK;
+}
+
+struct Span {
+  const void* p;
+  size_t bytes;
+};
+
+bool overlaps(Span a, Span b) {
+  if (!a.p || !b.p) return false;
+  const char* a0 = static_cast<const char*>(a.p);
+  const char* b0 = static_cast<const char*>(b.p);
+  return a0 < b0 + b.bytes && b0 < a0 + a.bytes;
+}
+
+int check_disjoint(const std::vector<Span>& ins, const std::vector<Span>& outs) {
+  for (size_t o = 0; o < outs.size(); ++o) {
+    for (const Span& i : ins)
+      if (overlaps(outs[o], i))
+        return fail(LFM_ERR_INVALID_ARG, "output buffer %zu overlaps an input buffer", o);
+    for (size_t o2 = o + 1; o2 < outs.size(); ++o2)
+      if (overlaps(outs[o], outs[o2]))
+        return fail(LFM_ERR_INVALID_ARG, "output buffers %zu and %zu overlap", o, o2);
+  }
+  return LFM_OK;
+}
+
+int run_step(lfm::StepArgs& a, cudaStream_t stream) {
+  int rc = status_word(&a.status);
+  if (rc) return rc;
+  const int path = g_path.load();
+  cudaError_t e = cudaErrorNotSupported;
+  if (path != 1) {
+    e = lfm::launch_tma_step(a, stream);
+    if (e != cudaSuccess && e != cudaErrorNotSupported) return cuda_fail(e, "fused step launch");
+    if (e == cudaErrorNotSupported && path == 2)
+      return fail(LFM_ERR_UNSUPPORTED, "no fused-kernel configuration for N=%d level=%d", a.N,
+                  a.level);
+  }
+  if (e == cudaErrorNotSupported) {
+    e = lfm::launch_direct_step(a, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "direct step launch");
+  }
+  return LFM_OK;
+}
+
+lfm::MaskLut device_lut(const float* table, const lfm_mask_lut* lut) {
+  lfm::MaskLut m;
+  m.table = table;
+  m.shift = lut->shift;
+  m.q_lo = lut->q_lo;
+  m.q_hi = lut->q_hi;
+  return m;
+}
+
+int check_lut(const float* table, const lfm_mask_lut* lut, int N) {
+  if (!lut) return fail(LFM_ERR_INVALID_ARG, "mask lookup table descriptor is null");
+  if (lut->N != N) return fail(LFM_ERR_INVALID_ARG, "lookup table is for N=%d, step N=%d", lut->N, N);
+  if (lut->count > 0 && !table) return fail(LFM_ERR_INVALID_ARG, "mask table pointer is null");
+  return LFM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// library context: cuFFT plans + spectrum scratch per lattice edge
+// ---------------------------------------------------------------------------
+struct FftSlot {
+  cufftHandle r2c = 0, c2r = 0;
+  float2* spec = nullptr;   // 3 * N * N * (N/2+1) complex
+  float* sa_raw = nullptr;  // 3 * N^3, for protocol colour steps
+};
+
+struct lfm_context {
+  int device = 0;
+  std::mutex mu;
+  std::map<int, FftSlot> slots;
+};
+
+namespace {
+
+int fft_slot(lfm_context* ctx, int N, bool need_sa_raw, FftSlot** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != ctx->device)
+    return fail(LFM_ERR_INVALID_ARG, "context belongs to device %d, current device is %d",
+                ctx->device, dev);
+  FftSlot& s = ctx->slots[N];
+  if (!s.spec) {
+    int n[3] = {N, N, N};
+    const int real_dist = N * N * N, cplx_dist = N * N * (N / 2 + 1);
+    if (cufftPlanMany(&s.r2c, 3, n, nullptr, 1, real_dist, nullptr, 1, cplx_dist, CUFFT_R2C, 3) !=
+        CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlanMany R2C N=%d", N);
+    if (cufftPlanMany(&s.c2r, 3, n, nullptr, 1, cplx_dist, nullptr, 1, real_dist, CUFFT_C2R, 3) !=
+        CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlanMany C2R N=%d", N);
+    e = cudaMalloc(&s.spec, sizeof(float2) * 3 * (size_t)cplx_dist);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc spectrum");
+  }
+  if (need_sa_raw && !s.sa_raw) {
+    e = cudaMalloc(&s.sa_raw, sizeof(float) * 3 * (size_t)N * N * N);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc S_a scratch");
+  }
+  *out = &s;
+  return LFM_OK;
+}
+
+int helmholtz(lfm_context* ctx, const float* pr, const float* pi, float* sa_raw, int N,
+              double gamma, double d, cudaStream_t stream, bool use_ctx_scratch,
+              float** sa_used) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  FftSlot* s = nullptr;
+  int rc = fft_slot(ctx, N, use_ctx_scratch, &s);
+  if (rc) return rc;
+  float* dst = use_ctx_scratch ? s->sa_raw : sa_raw;
+  cudaError_t e = lfm::launch_color_energy(pr, pi, dst, N, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "|Psi_a|^2 launch");
+  if (cufftSetStream(s->r2c, stream) != CUFFT_SUCCESS ||
+      cufftExecR2C(s->r2c, dst, reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
+    return fail(LFM_ERR_CUFFT, "cufftExecR2C N=%d", N);
+  e = lfm::launch_helmholtz_multiply_gd(s->spec, N, gamma, d, stream);
+  if (e != cudaSuccess) return cuda_fail(e, "Helmholtz multiply launch");
+  if (cufftSetStream(s->c2r, stream) != CUFFT_SUCCESS ||
+      cufftExecC2R(s->c2r, reinterpret_cast<cufftComplex*>(s->spec), dst) != CUFFT_SUCCESS)
+    return fail(LFM_ERR_CUFFT, "cufftExecC2R N=%d", N);
+  if (sa_used) *sa_used = dst;
+  return LFM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lfm_strerror(int status) {
+  switch (status) {
+    case LFM_OK: return "ok";
+    case LFM_ERR_INVALID_ARG: return "invalid argument";
+    case LFM_ERR_ALIGNMENT: return "device pointer not 16-byte aligned";
+    case LFM_ERR_UNSUPPORTED: return "unsupported configuration";
+    case LFM_ERR_CUDA: return "CUDA error";
+    case LFM_ERR_CUFFT: return "cuFFT error";
+    case LFM_ERR_MASK: return "mask is not a function of the radial key";
+    case LFM_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    case LFM_ERR_NONFINITE: return "non-finite value";
+    case LFM_ERR_CAPACITY: return "capacity exceeded";
+    default: return "unknown status";
+  }
+}
+
+const char* lfm_last_error_detail(void) { return t_detail.c_str(); }
+
+int lfm_abi_version(void) { return LFM_B200_ABI_VERSION; }
+
+int lfm_set_step_path(int path) {
+  if (path < 0 || path > 2) return fail(LFM_ERR_INVALID_ARG, "path %d not in {0,1,2}", path);
+  g_path.store(path);
+  return LFM_OK;
+}
+
+int lfm_mask_lut_build(int N, const float* mask_host, float* table_host, int capacity,
+                       lfm_mask_lut* out) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!mask_host || !out) return fail(LFM_ERR_INVALID_ARG, "null mask or descriptor");
+  const int shift = (N % 2 == 0) ? 3 : 2;
+  int32_t q_lo = INT32_MAX, q_hi = INT32_MIN;
+  // Pass 1: the band of keys whose mask is neither exactly 0 nor exactly 1.
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
+      for (int k = 0; k < N; ++k) {
+        const int32_t di = 2 * i - N + 1, dj = 2 * j - N + 1, dk = 2 * k - N + 1;
+        const int32_t q = di * di + dj * dj + dk * dk;
+        const float m = mask_host[((int64_t)i * N + j) * N + k];
+        if (m != 0.0f) q_lo = std::min(q_lo, q);
+        if (m != 1.0f) q_hi = std::max(q_hi, q);
+      }
+  lfm_mask_lut d;
+  d.N = N;
+  d.shift = shift;
+  if (q_lo == INT32_MAX) {  // mask identically 0
+    d.q_lo = INT32_MAX;
+    d.q_hi = INT32_MAX;
+    d.count = 0;
+  } else if (q_hi == INT32_MIN) {  // mask identically 1
+    d.q_lo = 0;
+    d.q_hi = -1;
+    d.count = 0;
+  } else {
+    d.q_lo = q_lo;
+    d.q_hi = q_hi;
+    d.count = q_hi >= q_lo ? ((q_hi - q_lo) >> shift) + 1 : 0;
+  }
+  if (d.count > capacity || (d.count > 0 && !table_host))
+    return fail(LFM_ERR_CAPACITY, "mask table needs %d entries, capacity %d", d.count, capacity);
+  // Pass 2: fill the band and check that equal keys carry equal values.
+  std::vector<uint8_t> seen(d.count, 0);
+  for (int i = 0; i < d.count; ++i) table_host[i] = 0.0f;
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j)
+      for (int k = 0; k < N; ++k) {
+        const int32_t di = 2 * i - N + 1, dj = 2 * j - N + 1, dk = 2 * k - N + 1;
+        const int32_t q = di * di + dj * dj + dk * dk;
+        const float m = mask_host[((int64_t)i * N + j) * N + k];
+        if (q < d.q_lo || q > d.q_hi) {
+          const float want = q < d.q_lo ? 0.0f : 1.0f;
+          if (memcmp(&m, &want, sizeof m) != 0)
+            return fail(LFM_ERR_MASK, "cell (%d,%d,%d) outside the band has mask %g", i, j, k, m);
+          continue;
+        }
+        if ((q - d.q_lo) & ((1 << shift) - 1))
+          return fail(LFM_ERR_MASK, "key %d off the 2^%d lattice", q, shift);
+        const int idx = (q - d.q_lo) >> shift;
+        if (seen[idx]) {
+          if (memcmp(&table_host[idx], &m, sizeof m) != 0)
+            return fail(LFM_ERR_MASK, "key %d has two mask values", q);
+        } else {
+          table_host[idx] = m;
+          seen[idx] = 1;
+        }
+      }
+  *out = d;
+  return LFM_OK;
+}
+
+int lfm_step_real_f32(const float* psi_in, const float* psi_prev_in, const float* chi_in,
+                      const float* chi_prev_in, const float* boundary_mask, float* psi_out,
+                      float* psi_prev_out, float* chi_out, float* chi_prev_out, int N,
+                      double dt2, double kappa, double lambda_self, double chi0, double e0_sq,
+                      void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_in || !psi_prev_in || !chi_in || !chi_prev_in || !boundary_mask || !psi_out ||
+      !psi_prev_out || !chi_out || !chi_prev_out)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_in, b}, {psi_prev_in, b}, {chi_in, b}, {chi_prev_in, b},
+                       {boundary_mask, b}},
+                      {{psi_out, b}, {psi_prev_out, b}, {chi_out, b}, {chi_prev_out, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_REAL;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, 0, 0, 0, 0, 0);
+  a.pr = psi_in; a.pr_prev = psi_prev_in; a.chi = chi_in; a.chi_prev = chi_prev_in;
+  a.pr_out = psi_out; a.pr_prev_out = psi_prev_out;
+  a.chi_out = chi_out; a.chi_prev_out = chi_prev_out;
+  a.mask = boundary_mask;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_step_complex_f32(const float* psi_r_in, const float* psi_r_prev_in,
+                         const float* psi_i_in, const float* psi_i_prev_in, const float* chi_in,
+                         const float* chi_prev_in, const float* boundary_mask,
+                         float* psi_r_out, float* psi_r_prev_out, float* psi_i_out,
+                         float* psi_i_prev_out, float* chi_out, float* chi_prev_out, int N,
+                         double dt2, double kappa, double lambda_self, double chi0,
+                         double e0_sq, double epsilon_w, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r_in || !psi_r_prev_in || !psi_i_in || !psi_i_prev_in || !chi_in || !chi_prev_in ||
+      !boundary_mask || !psi_r_out || !psi_r_prev_out || !psi_i_out || !psi_i_prev_out ||
+      !chi_out || !chi_prev_out)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r_in, b}, {psi_r_prev_in, b}, {psi_i_in, b}, {psi_i_prev_in, b},
+                       {chi_in, b}, {chi_prev_in, b}, {boundary_mask, b}},
+                      {{psi_r_out, b}, {psi_r_prev_out, b}, {psi_i_out, b}, {psi_i_prev_out, b},
+                       {chi_out, b}, {chi_prev_out, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COMPLEX;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, 0, 0, 0, 0);
+  a.pr = psi_r_in; a.pr_prev = psi_r_prev_in; a.pi = psi_i_in; a.pi_prev = psi_i_prev_in;
+  a.chi = chi_in; a.chi_prev = chi_prev_in;
+  a.pr_out = psi_r_out; a.pr_prev_out = psi_r_prev_out;
+  a.pi_out = psi_i_out; a.pi_prev_out = psi_i_prev_out;
+  a.chi_out = chi_out; a.chi_prev_out = chi_prev_out;
+  a.mask = boundary_mask;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_step_color_f32(lfm_context* ctx, const float* psi_r_in, const float* psi_r_prev_in,
+                       const float* psi_i_in, const float* psi_i_prev_in, const float* chi_in,
+                       const float* chi_prev_in, const float* boundary_mask, float* psi_r_out,
+                       float* psi_r_prev_out, float* psi_i_out, float* psi_i_prev_out,
+                       float* chi_out, float* chi_prev_out, int N, double dt2, double kappa,
+                       double lambda_self, double chi0, double e0_sq, double epsilon_w,
+                       double kappa_c, double epsilon_cc, double kappa_string,
+                       double kappa_tube, const float* sa_fields_in, float* sa_fields_out,
+                       double sa_gamma, double sa_d, double dt, void* stream) {
+  (void)sa_fields_in;  // recomputed from psi when used (numpy_backend.py:341-356)
+  (void)dt;
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r_in || !psi_r_prev_in || !psi_i_in || !psi_i_prev_in || !chi_in || !chi_prev_in ||
+      !boundary_mask || !psi_r_out || !psi_r_prev_out || !psi_i_out || !psi_i_prev_out ||
+      !chi_out || !chi_prev_out)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  const size_t b = sizeof(float) * (size_t)N * N * N, b3 = 3 * b;
+  const bool use_sa = kappa_tube > 0.0 && sa_fields_out != nullptr;
+  rc = check_disjoint({{psi_r_in, b3}, {psi_r_prev_in, b3}, {psi_i_in, b3}, {psi_i_prev_in, b3},
+                       {chi_in, b}, {chi_prev_in, b}, {boundary_mask, b}},
+                      {{psi_r_out, b3}, {psi_r_prev_out, b3}, {psi_i_out, b3},
+                       {psi_i_prev_out, b3}, {chi_out, b}, {chi_prev_out, b},
+                       {use_sa ? sa_fields_out : nullptr, b3}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COLOR;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, kappa_c,
+                              epsilon_cc, kappa_string, kappa_tube);
+  a.pr = psi_r_in; a.pr_prev = psi_r_prev_in; a.pi = psi_i_in; a.pi_prev = psi_i_prev_in;
+  a.chi = chi_in; a.chi_prev = chi_prev_in;
+  a.pr_out = psi_r_out; a.pr_prev_out = psi_r_prev_out;
+  a.pi_out = psi_i_out; a.pi_prev_out = psi_i_prev_out;
+  a.chi_out = chi_out; a.chi_prev_out = chi_prev_out;
+  a.mask = boundary_mask;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (use_sa) {
+    if (!ctx) return fail(LFM_ERR_INVALID_ARG, "kappa_tube > 0 needs a library context");
+    float* sa_raw = nullptr;
+    rc = helmholtz(ctx, psi_r_in, psi_i_in, nullptr, N, sa_gamma, sa_d, st, true, &sa_raw);
+    if (rc) return rc;
+    a.sa = sa_raw;
+    a.sa_clip_out = sa_fields_out;
+  }
+  return run_step(a, st);
+}
+
+int lfm_context_create(lfm_context** out) {
+  if (!out) return fail(LFM_ERR_INVALID_ARG, "null output");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  lfm_context* c = new lfm_context;
+  c->device = dev;
+  *out = c;
+  return LFM_OK;
+}
+
+int lfm_context_destroy(lfm_context* ctx) {
+  if (!ctx) return LFM_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->device);
+  for (auto& kv : ctx->slots) {
+    if (kv.second.r2c) cufftDestroy(kv.second.r2c);
+    if (kv.second.c2r) cufftDestroy(kv.second.c2r);
+    if (kv.second.spec) cudaFree(kv.second.spec);
+    if (kv.second.sa_raw) cudaFree(kv.second.sa_raw);
+  }
+  cudaSetDevice(prev);
+  delete ctx;
+  return LFM_OK;
+}
+
+int lfm_leapfrog_real_f32(const float* psi, float* psi_prev_io, const float* chi,
+                          float* chi_prev_io, const float* mask_table, const lfm_mask_lut* lut,
+                          int damp_prev, int N, double dt2, double kappa, double lambda_self,
+                          double chi0, double e0_sq, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi || !psi_prev_io || !chi || !chi_prev_io) return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi, b}, {chi, b}}, {{psi_prev_io, b}, {chi_prev_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_REAL;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, 0, 0, 0, 0, 0);
+  a.pr = psi; a.pr_prev = psi_prev_io; a.pr_out = psi_prev_io;
+  a.chi = chi; a.chi_prev = chi_prev_io; a.chi_out = chi_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_leapfrog_complex_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                             float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                             const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                             int N, double dt2, double kappa, double lambda_self, double chi0,
+                             double e0_sq, double epsilon_w, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r || !psi_r_prev_io || !psi_i || !psi_i_prev_io || !chi || !chi_prev_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r, b}, {psi_i, b}, {chi, b}},
+                      {{psi_r_prev_io, b}, {psi_i_prev_io, b}, {chi_prev_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COMPLEX;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, 0, 0, 0, 0);
+  a.pr = psi_r; a.pr_prev = psi_r_prev_io; a.pr_out = psi_r_prev_io;
+  a.pi = psi_i; a.pi_prev = psi_i_prev_io; a.pi_out = psi_i_prev_io;
+  a.chi = chi; a.chi_prev = chi_prev_io; a.chi_out = chi_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                           float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                           const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                           int N, double dt2, double kappa, double lambda_self, double chi0,
+                           double e0_sq, double epsilon_w, double kappa_c, double epsilon_cc,
+                           double kappa_string, double kappa_tube, const float* sa,
+                           void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r || !psi_r_prev_io || !psi_i || !psi_i_prev_io || !chi || !chi_prev_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N, b3 = 3 * b;
+  rc = check_disjoint({{psi_r, b3}, {psi_i, b3}, {chi, b}, {sa, sa ? b3 : 0}},
+                      {{psi_r_prev_io, b3}, {psi_i_prev_io, b3}, {chi_prev_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COLOR;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, kappa_c,
+                              epsilon_cc, kappa_string, kappa_tube);
+  a.pr = psi_r; a.pr_prev = psi_r_prev_io; a.pr_out = psi_r_prev_io;
+  a.pi = psi_i; a.pi_prev = psi_i_prev_io; a.pi_out = psi_i_prev_io;
+  a.chi = chi; a.chi_prev = chi_prev_io; a.chi_out = chi_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  a.sa = (kappa_tube > 0.0) ? sa : nullptr;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
+                         float* sa_raw, int N, double sa_gamma, double sa_d, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!ctx || !psi_r || !psi_i || !sa_raw) return fail(LFM_ERR_INVALID_ARG, "null argument");
+  const size_t b3 = 3 * sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r, b3}, {psi_i, b3}}, {{sa_raw, b3}});
+  if (rc) return rc;
+  return helmholtz(ctx, psi_r, psi_i, sa_raw, N, sa_gamma, sa_d,
+                   static_cast<cudaStream_t>(stream), false, nullptr);
+}
+
+int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* stream) {
+  if (!sa_raw || !sa_out || count < 0) return fail(LFM_ERR_INVALID_ARG, "bad argument");
+  if (count == 0) return LFM_OK;
+  cudaError_t e = lfm::launch_clip(sa_raw, sa_out, count, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "clip launch");
+  return LFM_OK;
+}
+
+int lfm_device_status(int* status_out, int clear) {
+  if (!status_out) return fail(LFM_ERR_INVALID_ARG, "null output");
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_lfm_status, sizeof v);
+  if (e != cudaSuccess) return cuda_fail(e, "read status word");
+  if (clear) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_lfm_status, &zero, sizeof zero);
+    if (e != cudaSuccess) return cuda_fail(e, "clear status word");
+  }
+  *status_out = v;
+  return LFM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// Per-cell updates of the three field levels, built from lfm_math.cuh.
+//
+// A kernel gathers the stencil values of a cell (S19) and the previous-step
+// values, then calls one of these.  The order of operations follows
+// lfm/core/backends/numpy_backend.py:80-382 line by line, so results are
+// bit-identical to the reference's NumPy float32 path.
+#pragma once
+
+#include "lfm_math.cuh"
+
+namespace lfm {
+
+// ---- REAL (numpy_backend.py:80-130) ---------------------------------------
+struct RealOut {
+  float psi, psi_prev, chi, chi_prev;
+};
+
+__device__ __forceinline__ RealOut real_cell(float lapE, float e, float e_prev, float lapX,
+                                             float chi, float chi_prev, float mask,
+                                             const StepConsts& s) {
+  const float chi_sq = fmul(chi, chi);
+  const float E_new = gov01(e, e_prev, lapE, chi_sq, s);
+  // chi_source = (kappa/chi0)*chi*(E*E - e0_sq)
+  const float src = fmul(fmul(s.k_over_chi0, chi), fsub(fmul(e, e), s.e0_sq));
+  float acc = fsub(lapX, src);
+  acc = mexican_hat(acc, chi, chi_sq, s);
+  const float absorb = fsub(1.0f, mask);
+  RealOut o;
+  o.psi = fmul(E_new, absorb);
+  o.psi_prev = fmul(e, absorb);
+  o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
+  o.chi_prev = chi;
+  return o;
+}
+
+// ---- COMPLEX (numpy_backend.py:132-205) -----------------------------------
+struct ComplexOut {
+  float pr, pr_prev, pi, pi_prev, chi, chi_prev;
+};
+
+// Face neighbours of one field, for the momentum current.
+struct Faces {
+  float im, ip, jm, jp, km, kp;
+};
+
+__device__ __forceinline__ float momentum_current(float pr, float pi, const Faces& R,
+                                                  const Faces& I) {
+  const float jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
+  const float jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
+  const float jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
+  return fmul(0.5f, fadd(fadd(jx, jy), jz));  // j_total = 0.5*(j_x + j_y + j_z)
+}
+
+__device__ __forceinline__ ComplexOut complex_cell(float lapR, float pr, float pr_prev,
+                                                   const Faces& R, float lapI, float pi,
+                                                   float pi_prev, const Faces& I, float lapX,
+                                                   float chi, float chi_prev, float mask,
+                                                   const StepConsts& s) {
+  const float chi_sq = fmul(chi, chi);
+  const float Pr_new = gov01(pr, pr_prev, lapR, chi_sq, s);
+  const float Pi_new = gov01(pi, pi_prev, lapI, chi_sq, s);
+  const float psi_sq = fadd(fmul(pr, pr), fmul(pi, pi));
+  const float jt = momentum_current(pr, pi, R, I);
+  // (kappa/chi0)*chi*(psi_sq + eps_w*j - e0_sq)
+  const float src =
+      fmul(fmul(s.k_over_chi0, chi), fsub(fadd(psi_sq, fmul(s.eps_w, jt)), s.e0_sq));
+  float acc = fsub(lapX, src);
+  acc = mexican_hat(acc, chi, chi_sq, s);
+  const float absorb = fsub(1.0f, mask);
+  ComplexOut o;
+  o.pr = fmul(Pr_new, absorb);
+  o.pi = fmul(Pi_new, absorb);
+  o.pr_prev = fmul(pr, absorb);
+  o.pi_prev = fmul(pi, absorb);
+  o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
+  o.chi_prev = chi;
+  return o;
+}
+
+// ---- COLOR (numpy_backend.py:207-382), three colours ----------------------
+// The colour step is split so a kernel can stream one colour at a time:
+// color_begin -> color_component (a = 0, 1, 2) -> color_finish.
+struct ColorAcc {
+  float chi, chi_sq, mask, absorb;
+  float pr_avg, pi_avg;
+  float psi_sq_total, j_total;
+  float ea[3];
+  float jd[3][3];  // per colour, per axis current (for CCV)
+};
+
+__device__ __forceinline__ void color_begin(ColorAcc& A, float chi, float mask,
+                                            const float pr_c[3], const float pi_c[3],
+                                            const StepConsts& s) {
+  A.chi = chi;
+  A.chi_sq = fmul(chi, chi);
+  A.mask = mask;
+  A.absorb = fsub(1.0f, mask);
+  A.pr_avg = 0.0f;
+  A.pi_avg = 0.0f;
+  if (s.use_cc) {  // Pr_avg = (0 + Pr_0 + Pr_1 + Pr_2) / 3   (numpy_backend.py:254-262)
+    float r = 0.0f, i = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      r = fadd(r, pr_c[a]);
+      i = fadd(i, pi_c[a]);
+    }
+    A.pr_avg = __fdiv_rn(r, 3.0f);
+    A.pi_avg = __fdiv_rn(i, 3.0f);
+  }
+  A.psi_sq_total = 0.0f;
+  A.j_total = 0.0f;
+}
+
+struct ColorCompOut {
+  float pr, pr_prev, pi, pi_prev;
+};
+
+// numpy_backend.py:268-310 for colour a.
+__device__ __forceinline__ ColorCompOut color_component(ColorAcc& A, int a, float lapR, float pr,
+                                                        float pr_prev, const Faces& R,
+                                                        float lapI, float pi, float pi_prev,
+                                                        const Faces& I, const StepConsts& s) {
+  float Pr_new = gov01(pr, pr_prev, lapR, A.chi_sq, s);
+  float Pi_new = gov01(pi, pi_prev, lapI, A.chi_sq, s);
+  if (s.use_cc) {  // -= dt2*eps_cc*chi^2*(Psi_a - Psi_bar)
+    const float t = fmul(s.dt2_eps_cc, A.chi_sq);
+    Pr_new = fsub(Pr_new, fmul(t, fsub(pr, A.pr_avg)));
+    Pi_new = fsub(Pi_new, fmul(t, fsub(pi, A.pi_avg)));
+  }
+  const float e = fadd(fmul(pr, pr), fmul(pi, pi));
+  A.ea[a] = e;
+  A.psi_sq_total = fadd(A.psi_sq_total, e);
+  const float jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
+  const float jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
+  const float jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
+  A.j_total = fadd(A.j_total, fmul(0.5f, fadd(fadd(jx, jy), jz)));
+  A.jd[a][0] = jx;
+  A.jd[a][1] = jy;
+  A.jd[a][2] = jz;
+  ColorCompOut o;
+  o.pr = fmul(Pr_new, A.absorb);
+  o.pi = fmul(Pi_new, A.absorb);
+  o.pr_prev = fmul(pr, A.absorb);
+  o.pi_prev = fmul(pi, A.absorb);
+  return o;
+}
+
+// f_c, CCV, SCV and GOV-02 (numpy_backend.py:312-370).  sa_raw holds the
+// unclipped S_a values of the cell (clipped here) or is ignored when
+// has_sa is false.  Returns the new chi.
+__device__ __forceinline__ float color_finish(const ColorAcc& A, float lapX, float chi_prev,
+                                              bool has_sa, const float sa_raw[3],
+                                              const StepConsts& s) {
+  const float third = (float)(1.0 / 3.0);
+  float color_var = 0.0f;
+  if (s.use_fc) {
+    float ssq = fadd(fmul(A.ea[0], A.ea[0]), fmul(A.ea[1], A.ea[1]));
+    ssq = fadd(ssq, fmul(A.ea[2], A.ea[2]));
+    const float tsq = fmul(A.psi_sq_total, A.psi_sq_total);
+    const bool safe = tsq > (float)1e-30;
+    // float32 quotient, then "- 1/3" in float64 (the float64 out array of
+    // np.divide), rounded back to float32.
+    const double ratio = safe ? (double)__fdiv_rn(ssq, tsq) : 0.0;
+    const float fc = __double2float_rn(__dmul_rn(__dsub_rn(ratio, 1.0 / 3.0), safe ? 1.0 : 0.0));
+    color_var = fmul(fmul(fmul(s.kc_over_chi0, A.chi), fc), A.psi_sq_total);
+  }
+  float ccv = 0.0f;
+  if (s.use_ccv) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float sq = fadd(fmul(A.jd[0][d], A.jd[0][d]), fmul(A.jd[1][d], A.jd[1][d]));
+      sq = fadd(sq, fmul(A.jd[2][d], A.jd[2][d]));
+      float sm = fadd(A.jd[0][d], A.jd[1][d]);
+      sm = fadd(sm, A.jd[2][d]);
+      ccv = fadd(ccv, fsub(sq, fmul(third, fmul(sm, sm))));
+    }
+  }
+  float scv = 0.0f;
+  if (has_sa) {
+    float ssum = 0.0f, ssq = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = fmaxf(sa_raw[a], 0.0f);  // np.clip(sa, 0, None)
+      ssum = fadd(ssum, v);
+      ssq = fadd(ssq, fmul(v, v));
+    }
+    scv = fsub(ssq, fmul(third, fmul(ssum, ssum)));
+  }
+  const float src =
+      fmul(fmul(s.k_over_chi0, A.chi), fsub(fadd(A.psi_sq_total, fmul(s.eps_w, A.j_total)), s.e0_sq));
+  float acc = fsub(lapX, src);
+  acc = fsub(acc, color_var);
+  acc = fsub(acc, fmul(s.kappa_string, ccv));
+  acc = fsub(acc, fmul(s.kappa_tube, scv));
+  acc = mexican_hat(acc, A.chi, A.chi_sq, s);
+  return gov02_finish(A.chi, chi_prev, acc, A.mask, A.absorb, s);
+}
+
+}  // namespace lfm

@@ -1,0 +1,52 @@
+// Internal interface between the C ABI (capi.cu) and the kernel files.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "lfm_math.cuh"
+
+namespace lfm {
+
+// Everything one step kernel launch needs.  Protocol mode: all *_out
+// pointers set, inputs and outputs distinct, mask = N^3 device array.
+// Resident mode: pr_out == pr_prev (and likewise pi, chi), the *_prev_out
+// pointers null, mask null and lut set.
+struct StepArgs {
+  int level;  // lfm_level
+  int N;
+  StepConsts c;
+  const float* pr;
+  const float* pi;
+  const float* chi;
+  const float* pr_prev;
+  const float* pi_prev;
+  const float* chi_prev;
+  float* pr_out;
+  float* pi_out;
+  float* chi_out;
+  float* pr_prev_out;
+  float* pi_prev_out;
+  float* chi_prev_out;
+  const float* mask;   // N^3 mask or null
+  MaskLut lut;         // used when mask is null
+  const float* sa;     // raw S_a (3*N^3) or null
+  float* sa_clip_out;  // clipped S_a copy (protocol colour step) or null
+  int damp_prev;       // multiply the previous-step fields by (1-mask) on read
+  int* status;         // device status word for bounded waits
+};
+
+cudaError_t launch_direct_step(const StepArgs& a, cudaStream_t stream);
+
+// Fused 2.5D kernel (N % 4 == 0).  Returns cudaErrorNotSupported when the
+// size has no tile configuration, so the caller can take the direct path.
+cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream);
+
+// S_a pipeline pieces (helmholtz.cu).
+cudaError_t launch_color_energy(const float* pr, const float* pi, float* e, int N,
+                                cudaStream_t stream);
+cudaError_t launch_helmholtz_multiply_gd(float2* spec, int N, double gamma, double d,
+                                         cudaStream_t stream);
+cudaError_t launch_clip(const float* in, float* out, int64_t count, cudaStream_t stream);
+
+}  // namespace lfm

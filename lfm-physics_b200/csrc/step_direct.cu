@@ -1,0 +1,158 @@
+// Direct step kernels: one thread per cell, neighbours read through L1.
+//
+// This is the general path: any N (odd sizes included), every level, both
+// the protocol (out-of-place, reference A/B semantics) and the resident
+// (in-place slot rotation) modes.  The fused 2.5D kernels in step_tma.cu
+// take over when N is a multiple of 4.
+#include "lfm_cells.cuh"
+#include "lfm_kernels.h"
+
+namespace lfm {
+namespace {
+
+struct Idx {
+  int64_t c, im, ip, jm, jp, km, kp;
+  int64_t imjm, imjp, ipjm, ipjp, imkm, imkp, ipkm, ipkp, jmkm, jmkp, jpkm, jpkp;
+};
+
+__device__ __forceinline__ Idx neighbour_index(int i, int j, int k, int N) {
+  const int64_t n = N;
+  const int64_t im = (i == 0 ? N - 1 : i - 1), ip = (i == N - 1 ? 0 : i + 1);
+  const int64_t jm = (j == 0 ? N - 1 : j - 1), jp = (j == N - 1 ? 0 : j + 1);
+  const int64_t km = (k == 0 ? N - 1 : k - 1), kp = (k == N - 1 ? 0 : k + 1);
+  const int64_t I0 = im * n * n, I1 = (int64_t)i * n * n, I2 = ip * n * n;
+  const int64_t J0 = jm * n, J1 = (int64_t)j * n, J2 = jp * n;
+  Idx x;
+  x.c = I1 + J1 + k;
+  x.im = I0 + J1 + k;   x.ip = I2 + J1 + k;
+  x.jm = I1 + J0 + k;   x.jp = I1 + J2 + k;
+  x.km = I1 + J1 + km;  x.kp = I1 + J1 + kp;
+  x.imjm = I0 + J0 + k; x.imjp = I0 + J2 + k; x.ipjm = I2 + J0 + k; x.ipjp = I2 + J2 + k;
+  x.imkm = I0 + J1 + km; x.imkp = I0 + J1 + kp; x.ipkm = I2 + J1 + km; x.ipkp = I2 + J1 + kp;
+  x.jmkm = I1 + J0 + km; x.jmkp = I1 + J0 + kp; x.jpkm = I1 + J2 + km; x.jpkp = I1 + J2 + kp;
+  return x;
+}
+
+__device__ __forceinline__ S19 gather(const float* __restrict__ f, const Idx& x) {
+  S19 s;
+  s.c = __ldg(f + x.c);
+  s.im = __ldg(f + x.im); s.ip = __ldg(f + x.ip);
+  s.jm = __ldg(f + x.jm); s.jp = __ldg(f + x.jp);
+  s.km = __ldg(f + x.km); s.kp = __ldg(f + x.kp);
+  s.imjm = __ldg(f + x.imjm); s.imjp = __ldg(f + x.imjp);
+  s.ipjm = __ldg(f + x.ipjm); s.ipjp = __ldg(f + x.ipjp);
+  s.imkm = __ldg(f + x.imkm); s.imkp = __ldg(f + x.imkp);
+  s.ipkm = __ldg(f + x.ipkm); s.ipkp = __ldg(f + x.ipkp);
+  s.jmkm = __ldg(f + x.jmkm); s.jmkp = __ldg(f + x.jmkp);
+  s.jpkm = __ldg(f + x.jpkm); s.jpkp = __ldg(f + x.jpkp);
+  return s;
+}
+
+__device__ __forceinline__ Faces faces_of(const S19& s) {
+  Faces f;
+  f.im = s.im; f.ip = s.ip; f.jm = s.jm; f.jp = s.jp; f.km = s.km; f.kp = s.kp;
+  return f;
+}
+
+__device__ __forceinline__ float cell_mask(const StepArgs& a, int i, int j, int k, int64_t x) {
+  if (a.mask) return __ldg(a.mask + x);
+  return mask_from_q(a.lut, qterm(i, a.N) + qterm(j, a.N) + qterm(k, a.N));
+}
+
+// Previous-step value: slots written by the previous resident step hold the
+// undamped field and get (1-mask) here, the same product the reference
+// stored (numpy_backend.py:128).
+__device__ __forceinline__ float prev_value(const StepArgs& a, const float* p, int64_t x,
+                                            float absorb) {
+  const float v = p[x];
+  return a.damp_prev ? fmul(v, absorb) : v;
+}
+
+template <int LEVEL>
+__global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
+  const int N = a.N;
+  const int64_t n3 = (int64_t)N * N * N;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n3;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(x % N);
+    const int j = (int)((x / N) % N);
+    const int i = (int)(x / ((int64_t)N * N));
+    const Idx ix = neighbour_index(i, j, k, N);
+    const float mask = cell_mask(a, i, j, k, x);
+    const float absorb = fsub(1.0f, mask);
+    const S19 X = gather(a.chi, ix);
+    const float chi_prev = a.chi_prev[x];
+    if (LEVEL == LFM_REAL) {
+      const S19 E = gather(a.pr, ix);
+      const RealOut o =
+          real_cell(lap19(E), E.c, prev_value(a, a.pr_prev, x, absorb), lap19(X), X.c, chi_prev,
+                    mask, a.c);
+      a.pr_out[x] = o.psi;
+      a.chi_out[x] = o.chi;
+      if (a.pr_prev_out) a.pr_prev_out[x] = o.psi_prev;
+      if (a.chi_prev_out) a.chi_prev_out[x] = o.chi_prev;
+    } else if (LEVEL == LFM_COMPLEX) {
+      const S19 R = gather(a.pr, ix);
+      const S19 I = gather(a.pi, ix);
+      const ComplexOut o = complex_cell(
+          lap19(R), R.c, prev_value(a, a.pr_prev, x, absorb), faces_of(R), lap19(I), I.c,
+          prev_value(a, a.pi_prev, x, absorb), faces_of(I), lap19(X), X.c, chi_prev, mask, a.c);
+      a.pr_out[x] = o.pr;
+      a.pi_out[x] = o.pi;
+      a.chi_out[x] = o.chi;
+      if (a.pr_prev_out) a.pr_prev_out[x] = o.pr_prev;
+      if (a.pi_prev_out) a.pi_prev_out[x] = o.pi_prev;
+      if (a.chi_prev_out) a.chi_prev_out[x] = o.chi_prev;
+    } else {
+      float pr_c[3], pi_c[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        pr_c[c] = __ldg(a.pr + c * n3 + x);
+        pi_c[c] = __ldg(a.pi + c * n3 + x);
+      }
+      ColorAcc A;
+      color_begin(A, X.c, mask, pr_c, pi_c, a.c);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const S19 R = gather(a.pr + c * n3, ix);
+        const S19 I = gather(a.pi + c * n3, ix);
+        const ColorCompOut o = color_component(
+            A, c, lap19(R), R.c, prev_value(a, a.pr_prev + c * n3, x, absorb), faces_of(R),
+            lap19(I), I.c, prev_value(a, a.pi_prev + c * n3, x, absorb), faces_of(I), a.c);
+        a.pr_out[c * n3 + x] = o.pr;
+        a.pi_out[c * n3 + x] = o.pi;
+        if (a.pr_prev_out) a.pr_prev_out[c * n3 + x] = o.pr_prev;
+        if (a.pi_prev_out) a.pi_prev_out[c * n3 + x] = o.pi_prev;
+      }
+      float sa[3] = {0.0f, 0.0f, 0.0f};
+      if (a.sa) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sa[c] = __ldg(a.sa + c * n3 + x);
+        if (a.sa_clip_out) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) a.sa_clip_out[c * n3 + x] = fmaxf(sa[c], 0.0f);
+        }
+      }
+      a.chi_out[x] = color_finish(A, lap19(X), chi_prev, a.sa != nullptr, sa, a.c);
+      if (a.chi_prev_out) a.chi_prev_out[x] = X.c;
+    }
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_direct_step(const StepArgs& a, cudaStream_t stream) {
+  const int64_t n3 = (int64_t)a.N * a.N * a.N;
+  const int block = 256;
+  int64_t blocks = (n3 + block - 1) / block;
+  const int64_t cap = 148LL * 16;  // grid-stride beyond 16 waves of CTAs
+  if (blocks > cap) blocks = cap;
+  switch (a.level) {
+    case LFM_REAL: direct_step_kernel<LFM_REAL><<<(int)blocks, block, 0, stream>>>(a); break;
+    case LFM_COMPLEX: direct_step_kernel<LFM_COMPLEX><<<(int)blocks, block, 0, stream>>>(a); break;
+    default: direct_step_kernel<LFM_COLOR><<<(int)blocks, block, 0, stream>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace lfm

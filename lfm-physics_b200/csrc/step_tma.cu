@@ -1,0 +1,599 @@
+// Fused 2.5D step kernels for sm_100a (N % 4 == 0).
+//
+// Layout: fields are C-order [i][j][k], k contiguous.  A CTA owns a tile of
+// TJ whole rows (j0 .. j0+TJ-1, every k) and marches along i over a chunk
+// of planes [i0, i1).  For each plane p the TMA engine copies, with 1-D bulk
+// copies (cp.async.bulk) completing on an mbarrier:
+//   * every stencil field (Psi components and chi): the TJ tile rows plus
+//     the two periodic halo rows j0-1 and j0+TJ -> TJ+2 rows of N floats;
+//   * every point field (previous-step fields, the protocol mask, S_a):
+//     the TJ tile rows.
+// into one stage of an S-deep shared-memory ring.  Computing plane i reads
+// the stages of planes i-1, i, i+1; after a CTA barrier the stage of i-1 is
+// refilled with plane i-1+S, so S-3 planes stream in while one is computed.
+// Periodic wrap in i and j is folded into the copy addresses; wrap in k is
+// resolved when reading shared memory.  Each thread updates V consecutive
+// cells of one row with vector loads/stores; its k-1 / k+V neighbours come
+// from the adjacent lanes by warp shuffle (shared memory at row ends and
+// warp edges).  Arithmetic: lfm_cells.cuh, bit-identical to the reference.
+//
+// Every mbarrier wait is bounded by wall time (%globaltimer); on timeout the
+// CTA records LFM_ERR_DEVICE_TIMEOUT in the status word, waits (bounded)
+// for its own copies in flight and returns.
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+
+#include "lfm_cells.cuh"
+#include "lfm_kernels.h"
+#include "lfm_tune.h"
+
+namespace lfm {
+namespace {
+
+constexpr int kMaxStencil = 7;
+constexpr int kMaxPoint = 11;
+constexpr int kMaxStages = 6;
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per wait
+constexpr uint64_t kDrainLimitNs = 100000000ull;  // 0.1 s per stage when draining
+
+struct TmaParams {
+  StepArgs a;
+  const float* sf[kMaxStencil];  // stencil fields (base of each component)
+  const float* pf[kMaxPoint];    // point fields
+  int ns, np;                    // counts
+  int pf_mask;                   // index of the mask point field, -1 = lookup table
+  int pf_sa;                     // index of S_a colour 0, -1 = none
+  int N, TJ, IC, S, JT;
+  int stage_floats;
+};
+
+// ---- PTX helpers -------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(float* dst, const float* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = now_ns();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (now_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// ---- vector helpers ------------------------------------------------------------
+template <int V>
+struct Vec {
+  float v[V];
+};
+
+template <int V>
+__device__ __forceinline__ Vec<V> lds(const float* smem, int off) {
+  Vec<V> r;
+  if constexpr (V == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(smem + off);
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else if constexpr (V == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(smem + off);
+    r.v[0] = t.x; r.v[1] = t.y;
+  } else {
+    r.v[0] = smem[off];
+  }
+  return r;
+}
+
+template <int V>
+__device__ __forceinline__ void stg(float* p, const float (&x)[V]) {
+  if constexpr (V == 4) {
+    *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(x[0], x[1]);
+  } else {
+    *p = x[0];
+  }
+}
+
+// Per-thread geometry inside the tile.
+struct Lane {
+  int r;        // tile row (0..TJ-1)
+  int k0;       // first k of the thread's V cells
+  int km1, kpv; // periodic k0-1 and k0+V
+  bool fix_l, fix_r;  // neighbour not in the adjacent lane: read shared memory
+};
+
+__device__ __forceinline__ float left_nb(float mine_last, const float* smem, int row_off,
+                                         const Lane& L) {
+  float v = __shfl_up_sync(0xffffffffu, mine_last, 1);
+  if (L.fix_l) v = smem[row_off + L.km1];
+  return v;
+}
+
+__device__ __forceinline__ float right_nb(float mine_first, const float* smem, int row_off,
+                                          const Lane& L) {
+  float v = __shfl_down_sync(0xffffffffu, mine_first, 1);
+  if (L.fix_r) v = smem[row_off + L.kpv];
+  return v;
+}
+
+// The 19-point stencil of one field for the thread's V cells.  fm/f0/fp are
+// the offsets of this field's TJ+2 rows in the stages of planes i-1, i, i+1
+// (row 0 = tile row -1).  Returns the Laplacian and centre per cell and, with
+// FACES, the six face neighbours (for the momentum current).
+template <int V, bool FACES>
+__device__ __forceinline__ void field_stencil(const float* smem, int fm, int f0, int fp, int N,
+                                              const Lane& L, float (&lap)[V], float (&ctr)[V],
+                                              Faces (&faces)[V]) {
+  const int rm = (L.r) * N, r0 = (L.r + 1) * N, rp = (L.r + 2) * N;
+  const Vec<V> A_m = lds<V>(smem, f0 + rm + L.k0);
+  const Vec<V> A_0 = lds<V>(smem, f0 + r0 + L.k0);
+  const Vec<V> A_p = lds<V>(smem, f0 + rp + L.k0);
+  const Vec<V> M_m = lds<V>(smem, fm + rm + L.k0);
+  const Vec<V> M_0 = lds<V>(smem, fm + r0 + L.k0);
+  const Vec<V> M_p = lds<V>(smem, fm + rp + L.k0);
+  const Vec<V> P_m = lds<V>(smem, fp + rm + L.k0);
+  const Vec<V> P_0 = lds<V>(smem, fp + r0 + L.k0);
+  const Vec<V> P_p = lds<V>(smem, fp + rp + L.k0);
+  const float A_m_l = left_nb(A_m.v[V - 1], smem, f0 + rm, L);
+  const float A_m_r = right_nb(A_m.v[0], smem, f0 + rm, L);
+  const float A_0_l = left_nb(A_0.v[V - 1], smem, f0 + r0, L);
+  const float A_0_r = right_nb(A_0.v[0], smem, f0 + r0, L);
+  const float A_p_l = left_nb(A_p.v[V - 1], smem, f0 + rp, L);
+  const float A_p_r = right_nb(A_p.v[0], smem, f0 + rp, L);
+  const float M_0_l = left_nb(M_0.v[V - 1], smem, fm + r0, L);
+  const float M_0_r = right_nb(M_0.v[0], smem, fm + r0, L);
+  const float P_0_l = left_nb(P_0.v[V - 1], smem, fp + r0, L);
+  const float P_0_r = right_nb(P_0.v[0], smem, fp + r0, L);
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    S19 s;
+    s.c = A_0.v[e];
+    s.im = M_0.v[e];
+    s.ip = P_0.v[e];
+    s.jm = A_m.v[e];
+    s.jp = A_p.v[e];
+    s.km = e > 0 ? A_0.v[e - 1] : A_0_l;
+    s.kp = e < V - 1 ? A_0.v[e + 1] : A_0_r;
+    s.imjm = M_m.v[e];
+    s.imjp = M_p.v[e];
+    s.ipjm = P_m.v[e];
+    s.ipjp = P_p.v[e];
+    s.imkm = e > 0 ? M_0.v[e - 1] : M_0_l;
+    s.imkp = e < V - 1 ? M_0.v[e + 1] : M_0_r;
+    s.ipkm = e > 0 ? P_0.v[e - 1] : P_0_l;
+    s.ipkp = e < V - 1 ? P_0.v[e + 1] : P_0_r;
+    s.jmkm = e > 0 ? A_m.v[e - 1] : A_m_l;
+    s.jmkp = e < V - 1 ? A_m.v[e + 1] : A_m_r;
+    s.jpkm = e > 0 ? A_p.v[e - 1] : A_p_l;
+    s.jpkp = e < V - 1 ? A_p.v[e + 1] : A_p_r;
+    lap[e] = lap19(s);
+    ctr[e] = s.c;
+    if (FACES) {
+      faces[e].im = s.im; faces[e].ip = s.ip;
+      faces[e].jm = s.jm; faces[e].jp = s.jp;
+      faces[e].km = s.km; faces[e].kp = s.kp;
+    }
+  }
+}
+
+template <int LEVEL, int V>
+__device__ __forceinline__ void compute_plane(const TmaParams& P, const float* smem, int sm,
+                                              int s0, int sp, int i, const Lane& L, int j) {
+  const StepArgs& a = P.a;
+  const int N = P.N, TJ = P.TJ;
+  const int field_rows = (TJ + 2) * N;
+  const int point_base = P.ns * field_rows;
+  const int pt = point_base + L.r * N + L.k0;  // + g*TJ*N for point field g
+  const int64_t gofs = ((int64_t)i * N + j) * N + L.k0;
+
+  // sponge factor per cell
+  float mask[V], absorb[V];
+  if (P.pf_mask >= 0) {
+    const Vec<V> m = lds<V>(smem, s0 + pt + P.pf_mask * TJ * N);
+#pragma unroll
+    for (int e = 0; e < V; ++e) mask[e] = m.v[e];
+  } else {
+    const int32_t qij = qterm(i, N) + qterm(j, N);
+#pragma unroll
+    for (int e = 0; e < V; ++e) mask[e] = mask_from_q(a.lut, qij + qterm(L.k0 + e, N));
+  }
+#pragma unroll
+  for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
+
+  auto prev = [&](int g, float (&out)[V]) {
+    const Vec<V> p = lds<V>(smem, s0 + pt + g * TJ * N);
+#pragma unroll
+    for (int e = 0; e < V; ++e) out[e] = a.damp_prev ? fmul(p.v[e], absorb[e]) : p.v[e];
+  };
+  auto plain = [&](int g, float (&out)[V]) {
+    const Vec<V> p = lds<V>(smem, s0 + pt + g * TJ * N);
+#pragma unroll
+    for (int e = 0; e < V; ++e) out[e] = p.v[e];
+  };
+
+  Faces nofaces[V];
+  if constexpr (LEVEL == LFM_REAL) {
+    float lapE[V], cE[V], lapX[V], cX[V], ep[V], xp[V];
+    field_stencil<V, false>(smem, sm, s0, sp, N, L, lapE, cE, nofaces);
+    field_stencil<V, false>(smem, sm + field_rows, s0 + field_rows, sp + field_rows, N, L, lapX,
+                            cX, nofaces);
+    prev(0, ep);
+    plain(1, xp);
+    float o_psi[V], o_chi[V], o_pp[V], o_cp[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const RealOut o = real_cell(lapE[e], cE[e], ep[e], lapX[e], cX[e], xp[e], mask[e], a.c);
+      o_psi[e] = o.psi; o_chi[e] = o.chi; o_pp[e] = o.psi_prev; o_cp[e] = o.chi_prev;
+    }
+    stg<V>(a.pr_out + gofs, o_psi);
+    stg<V>(a.chi_out + gofs, o_chi);
+    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_pp);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
+  } else if constexpr (LEVEL == LFM_COMPLEX) {
+    float lapR[V], cR[V], lapI[V], cI[V], lapX[V], cX[V], rp[V], ip[V], xp[V];
+    Faces fR[V], fI[V];
+    field_stencil<V, true>(smem, sm, s0, sp, N, L, lapR, cR, fR);
+    field_stencil<V, true>(smem, sm + field_rows, s0 + field_rows, sp + field_rows, N, L, lapI,
+                           cI, fI);
+    field_stencil<V, false>(smem, sm + 2 * field_rows, s0 + 2 * field_rows, sp + 2 * field_rows,
+                            N, L, lapX, cX, nofaces);
+    prev(0, rp);
+    prev(1, ip);
+    plain(2, xp);
+    float o_r[V], o_i[V], o_c[V], o_rp[V], o_ip[V], o_cp[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const ComplexOut o = complex_cell(lapR[e], cR[e], rp[e], fR[e], lapI[e], cI[e], ip[e],
+                                        fI[e], lapX[e], cX[e], xp[e], mask[e], a.c);
+      o_r[e] = o.pr; o_i[e] = o.pi; o_c[e] = o.chi;
+      o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev; o_cp[e] = o.chi_prev;
+    }
+    stg<V>(a.pr_out + gofs, o_r);
+    stg<V>(a.pi_out + gofs, o_i);
+    stg<V>(a.chi_out + gofs, o_c);
+    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_rp);
+    if (a.pi_prev_out) stg<V>(a.pi_prev_out + gofs, o_ip);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
+  } else {
+    const int64_t n3 = (int64_t)N * N * N;
+    // stencil fields: R0 R1 R2 I0 I1 I2 chi ; point fields: Rp0..2 Ip0..2 chip [mask] [S0..2]
+    float lapX[V], cX[V], xp[V];
+    field_stencil<V, false>(smem, sm + 6 * field_rows, s0 + 6 * field_rows, sp + 6 * field_rows,
+                            N, L, lapX, cX, nofaces);
+    plain(6, xp);
+    ColorAcc A[V];
+    {
+      Vec<V> cr[3], ci[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cr[c] = lds<V>(smem, s0 + c * field_rows + (L.r + 1) * N + L.k0);
+        ci[c] = lds<V>(smem, s0 + (3 + c) * field_rows + (L.r + 1) * N + L.k0);
+      }
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
+        const float pic[3] = {ci[0].v[e], ci[1].v[e], ci[2].v[e]};
+        color_begin(A[e], cX[e], mask[e], prc, pic, a.c);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float lapR[V], cR[V], lapI[V], cI[V], rp[V], ip[V];
+      Faces fR[V], fI[V];
+      field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
+                             N, L, lapR, cR, fR);
+      field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
+                             sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
+      prev(c, rp);
+      prev(3 + c, ip);
+      float o_r[V], o_i[V], o_rp[V], o_ip[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const ColorCompOut o =
+            color_component(A[e], c, lapR[e], cR[e], rp[e], fR[e], lapI[e], cI[e], ip[e], fI[e],
+                            a.c);
+        o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
+      }
+      stg<V>(a.pr_out + c * n3 + gofs, o_r);
+      stg<V>(a.pi_out + c * n3 + gofs, o_i);
+      if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
+      if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
+    }
+    float sa[V][3];
+    const bool has_sa = P.pf_sa >= 0;
+    if (has_sa) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float t[V];
+        plain(P.pf_sa + c, t);
+#pragma unroll
+        for (int e = 0; e < V; ++e) sa[e][c] = t[e];
+        if (a.sa_clip_out) {
+#pragma unroll
+          for (int e = 0; e < V; ++e) t[e] = fmaxf(t[e], 0.0f);
+          stg<V>(a.sa_clip_out + c * n3 + gofs, t);
+        }
+      }
+    }
+    float o_c[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) o_c[e] = color_finish(A[e], lapX[e], xp[e], has_sa, sa[e], a.c);
+    stg<V>(a.chi_out + gofs, o_c);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
+  }
+}
+
+// Copies plane (i0 - 1 + u) into stage u % S.
+__device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uint64_t* bars,
+                                            int u, int i0, int i1, int j0) {
+  const int N = P.N, TJ = P.TJ;
+  const int p = i0 - 1 + u;
+  const int pw = (p % N + N) % N;
+  const int s = u % P.S;
+  float* st = smem + (size_t)s * P.stage_floats;
+  const bool point = (p >= i0) && (p < i1);
+  const uint32_t row_bytes = 4u * (uint32_t)N;
+  const uint32_t bytes =
+      row_bytes * (uint32_t)(P.ns * (TJ + 2) + (point ? P.np * TJ : 0));
+  mbar_expect_tx(&bars[s], bytes);
+  const int jm = (j0 == 0) ? N - 1 : j0 - 1;
+  const int jp = (j0 + TJ == N) ? 0 : j0 + TJ;
+  const int64_t plane = (int64_t)pw * N;
+  for (int f = 0; f < P.ns; ++f) {
+    float* d = st + (size_t)f * (TJ + 2) * N;
+    const float* g = P.sf[f];
+    bulk_copy_g2s(d + N, g + (plane + j0) * N, row_bytes * TJ, &bars[s]);
+    bulk_copy_g2s(d, g + (plane + jm) * N, row_bytes, &bars[s]);
+    bulk_copy_g2s(d + (size_t)(TJ + 1) * N, g + (plane + jp) * N, row_bytes, &bars[s]);
+  }
+  if (point) {
+    float* base = st + (size_t)P.ns * (TJ + 2) * N;
+    for (int g = 0; g < P.np; ++g)
+      bulk_copy_g2s(base + (size_t)g * TJ * N, P.pf[g] + (plane + j0) * N, row_bytes * TJ,
+                    &bars[s]);
+  }
+}
+
+template <int LEVEL, int V>
+__global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ TmaParams P) {
+  extern __shared__ __align__(128) float smem[];
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  __shared__ int abort_flag;
+
+  const int N = P.N, TJ = P.TJ, S = P.S;
+  const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
+  const int j0 = jt * TJ;
+  const int i0 = ch * P.IC;
+  const int i1 = min(i0 + P.IC, N);
+  const int nplanes = (i1 - i0) + 2;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int tpr = N / V;
+
+  Lane L;
+  L.r = tid / tpr;
+  const int kv = tid % tpr;
+  L.k0 = kv * V;
+  L.km1 = (L.k0 == 0) ? N - 1 : L.k0 - 1;
+  L.kpv = (L.k0 + V == N) ? 0 : L.k0 + V;
+  L.fix_l = (lane == 0) || (kv == 0);
+  L.fix_r = (lane == 31) || (kv == tpr - 1);
+  const int j = j0 + L.r;
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+    abort_flag = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  int issued = 0;
+  if (tid == 0) {
+    for (; issued < min(S, nplanes); ++issued) issue_plane(P, smem, bars, issued, i0, i1, j0);
+  }
+
+  int waited = 0;
+  for (int c = 0; c < i1 - i0; ++c) {
+    bool ok = true;
+    while (waited <= c + 2) {
+      ok = ok && mbar_wait_bounded(&bars[waited % S], (uint32_t)((waited / S) & 1), kWaitLimitNs);
+      ++waited;
+    }
+    if (!ok) {
+      abort_flag = 1;
+      atomicOr(P.a.status, LFM_ERR_DEVICE_TIMEOUT);
+    } else {
+      const int sf = P.stage_floats;
+      compute_plane<LEVEL, V>(P, smem, (c % S) * sf, ((c + 1) % S) * sf, ((c + 2) % S) * sf,
+                              i0 + c, L, j);
+    }
+    __syncthreads();
+    if (abort_flag) break;
+    if (tid == 0 && c + S < nplanes) {
+      issue_plane(P, smem, bars, c + S, i0, i1, j0);
+      issued = c + S + 1;
+    }
+  }
+  if (abort_flag && tid == 0) {
+    // Let the copies this CTA started finish before its shared memory goes away.
+    for (int u = waited; u < issued; ++u)
+      mbar_wait_bounded(&bars[u % S], (uint32_t)((u / S) & 1), kDrainLimitNs);
+  }
+}
+
+// ---- host side -------------------------------------------------------------------
+struct Choice {
+  int TJ = 0, S = 0, IC = 0, threads = 0, smem = 0;
+};
+
+constexpr int kSmemLimit = 227 * 1024;
+
+int stage_bytes(int N, int TJ, int ns, int np) { return 4 * N * (ns * (TJ + 2) + np * TJ); }
+
+Choice choose(int level, int N, int V, int ns, int np) {
+  Choice best;
+  double best_score = -1.0;
+  const int tpr = N / V;
+  TileConfig forced;
+  const bool have_forced = tune_lookup(level, N, &forced);
+  for (int TJ = 1; TJ <= N; ++TJ) {
+    if (N % TJ) continue;
+    const int threads = TJ * tpr;
+    if (threads % 32 || threads < 64 || threads > 512) continue;
+    for (int S = 4; S <= kMaxStages; ++S) {
+      const int smem = S * stage_bytes(N, TJ, ns, np);
+      if (smem > kSmemLimit) continue;
+      if (have_forced && (forced.tj != TJ || forced.stages != S)) continue;
+      const int cta_by_smem = (228 * 1024) / (smem + 1024);
+      const int cta_by_thr = 2048 / threads;
+      const int ctas = std::max(1, std::min(cta_by_smem, cta_by_thr));
+      const double warps = std::min(ctas * threads / 32, 48);
+      const double halo = (double)TJ / (TJ + 2);            // useful fraction of stencil rows
+      const double depth = std::min(S - 3, 2) / 2.0;        // planes streamed ahead
+      const double score = warps / 48.0 + 0.6 * halo + 0.25 * depth;
+      if (score > best_score) {
+        best_score = score;
+        best.TJ = TJ;
+        best.S = S;
+        best.threads = threads;
+        best.smem = smem;
+      }
+    }
+  }
+  if (!best.TJ) return best;
+  const int JT = N / best.TJ;
+  const int ctas = std::max(1, std::min((228 * 1024) / (best.smem + 1024), 2048 / best.threads));
+  if (have_forced && forced.ic > 0) {
+    best.IC = std::min(forced.ic, N);
+  } else {
+    // about four waves of tiles over 148 SMs, at least 8 planes per chunk
+    const long target_tiles = 4L * 148 * ctas;
+    int ic = (int)(((long)N * JT + target_tiles - 1) / target_tiles);
+    best.IC = std::max(8, std::min(ic, N));
+  }
+  return best;
+}
+
+template <int LEVEL, int V>
+cudaError_t launch_level(const TmaParams& P, const Choice& ch, cudaStream_t stream) {
+  static std::once_flag once;
+  static cudaError_t attr_err = cudaSuccess;
+  std::call_once(once, [] {
+    attr_err = cudaFuncSetAttribute(tma_step_kernel<LEVEL, V>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit);
+  });
+  if (attr_err != cudaSuccess) return attr_err;
+  const int JT = P.N / P.TJ;
+  const int chunks = (P.N + P.IC - 1) / P.IC;
+  tma_step_kernel<LEVEL, V><<<JT * chunks, ch.threads, ch.smem, stream>>>(P);
+  return cudaGetLastError();
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
+  const int N = a.N;
+  if (N % 4 != 0 || N < 8) return cudaErrorNotSupported;
+  const int V = (a.level == LFM_COLOR) ? 2 : 4;
+  TmaParams P{};
+  P.a = a;
+  P.N = N;
+  P.pf_mask = -1;
+  P.pf_sa = -1;
+  const int64_t n3 = (int64_t)N * N * N;
+  if (a.level == LFM_REAL) {
+    P.ns = 2;
+    P.sf[0] = a.pr; P.sf[1] = a.chi;
+    P.pf[0] = a.pr_prev; P.pf[1] = a.chi_prev;
+    P.np = 2;
+  } else if (a.level == LFM_COMPLEX) {
+    P.ns = 3;
+    P.sf[0] = a.pr; P.sf[1] = a.pi; P.sf[2] = a.chi;
+    P.pf[0] = a.pr_prev; P.pf[1] = a.pi_prev; P.pf[2] = a.chi_prev;
+    P.np = 3;
+  } else {
+    P.ns = 7;
+    for (int c = 0; c < 3; ++c) {
+      P.sf[c] = a.pr + c * n3;
+      P.sf[3 + c] = a.pi + c * n3;
+      P.pf[c] = a.pr_prev + c * n3;
+      P.pf[3 + c] = a.pi_prev + c * n3;
+    }
+    P.sf[6] = a.chi;
+    P.pf[6] = a.chi_prev;
+    P.np = 7;
+  }
+  if (a.mask) {
+    P.pf_mask = P.np;
+    P.pf[P.np++] = a.mask;
+  }
+  if (a.level == LFM_COLOR && a.sa) {
+    P.pf_sa = P.np;
+    for (int c = 0; c < 3; ++c) P.pf[P.np++] = a.sa + c * n3;
+  }
+  // every copy source and every vector store needs 16-byte alignment
+  const void* ptrs[] = {a.pr, a.pi, a.chi, a.pr_prev, a.pi_prev, a.chi_prev, a.pr_out, a.pi_out,
+                        a.chi_out, a.pr_prev_out, a.pi_prev_out, a.chi_prev_out, a.mask, a.sa,
+                        a.sa_clip_out};
+  for (const void* p : ptrs)
+    if (p && !aligned16(p)) return cudaErrorNotSupported;
+
+  const Choice ch = choose(a.level, N, V, P.ns, P.np);
+  if (!ch.TJ) return cudaErrorNotSupported;
+  P.TJ = ch.TJ;
+  P.S = ch.S;
+  P.IC = ch.IC;
+  P.JT = N / ch.TJ;
+  P.stage_floats = ch.smem / (4 * ch.S);
+  tune_record(a.level, N, TileConfig{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem});
+  switch (a.level) {
+    case LFM_REAL: return launch_level<LFM_REAL, 4>(P, ch, stream);
+    case LFM_COMPLEX: return launch_level<LFM_COMPLEX, 4>(P, ch, stream);
+    default: return launch_level<LFM_COLOR, 2>(P, ch, stream);
+  }
+}
+
+}  // namespace lfm

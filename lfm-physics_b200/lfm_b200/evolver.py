@@ -1,0 +1,384 @@
+"""Double-buffered evolver on the B200 library.
+
+Public API of the reference ``Evolver`` (lfm/core/evolver.py:42-536):
+``Evolver(config, backend=...)``, ``evolve(steps, callback, freeze_chi)``,
+``get_*`` / ``set_*`` field accessors, ``step``, ``_use_buffer_A`` and the
+buffer attributes ``psi_r_A`` ... ``chi_prev_B`` / ``sa_A`` that hooks use.
+
+Two buffer layouts, identical results bit for bit:
+
+``buffers="resident"`` (default)
+    Two slots per field.  Each step reads (cur, prev) and writes the new
+    field over prev (lfm_leapfrog_*_f32), 24 B/cell at REAL.  The stored
+    prev then holds the undamped field and the kernel applies the sponge
+    factor on read -- the same float32 product the reference stores
+    (numpy_backend.py:128), so nothing changes in the results.  The mask
+    comes from the radial lookup table.
+
+``buffers="ab"``
+    The reference's four-buffer A/B layout (evolver.py:87-135), stepped
+    through the protocol calls (lfm_step_*_f32), for callers that need every
+    A/B buffer to hold exactly what the reference's would.
+
+COLOR with kappa_tube > 0 runs the S_a Helmholtz solve (cuFFT) from the
+current Psi before each step, as numpy_backend.py:341-356 does.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .backend import B200Backend, _stream_handle, get_backend
+from .config import FieldLevel
+from .mask import MaskTable, boundary_mask as host_boundary_mask
+
+
+class Evolver:
+    """Leapfrog evolver for one lattice on one GPU."""
+
+    def __init__(self, config, backend="auto", buffers: str = "resident") -> None:
+        import torch
+
+        self.config = config
+        self.backend = backend if isinstance(backend, B200Backend) else get_backend(backend)
+        self.device = self.backend.device
+        self.N = int(config.grid_size)
+        self.total = self.N**3
+        self.step = 0
+        self._use_buffer_A = True
+        self._level = FieldLevel(int(config.field_level))
+        if buffers not in ("resident", "ab"):
+            raise ValueError(f"buffers must be 'resident' or 'ab', got {buffers!r}")
+        self._mode = buffers
+        if self._level == FieldLevel.COLOR and int(config.n_colors) != 3:
+            # The reference kernels hard-code three colours (numpy_backend.py:240,
+            # kernel_source.py:107) whatever n_colors says; refuse instead.
+            raise ValueError(f"COLOR level steps exactly 3 colours, config has n_colors="
+                             f"{config.n_colors}")
+        self._n_psi = 1 if self._level != FieldLevel.COLOR else 3
+        self._has_imag = self._level != FieldLevel.REAL
+        self._dt2 = config.dt**2
+        self._N = self.N
+        self._sa_on = bool(config.kappa_tube > 0.0) and self._level == FieldLevel.COLOR
+
+        N, n = self.N, self.total
+        psi_n = self._n_psi * n
+        f32 = dict(dtype=torch.float32, device=self.device)
+        mask_np = host_boundary_mask(N, config.boundary_fraction)
+        self.boundary_mask = torch.from_numpy(mask_np).to(self.device)
+        self._absorb = 1.0 - self.boundary_mask  # float32, as numpy_backend.py:122
+        if self._level == FieldLevel.COLOR:
+            self._absorb_psi = self._absorb.repeat(3)
+        else:
+            self._absorb_psi = self._absorb
+
+        if self._mode == "resident":
+            self._table = MaskTable.from_mask(N, mask_np)
+            self._table_dev = self._table.to_device(self.device)
+            self._desc = self._table.desc
+            self._pr = [torch.zeros(psi_n, **f32), torch.zeros(psi_n, **f32)]
+            self._pi = ([torch.zeros(psi_n, **f32), torch.zeros(psi_n, **f32)]
+                        if self._has_imag else [None, None])
+            self._chi = [torch.full((n,), float(config.chi0), **f32) for _ in range(2)]
+            self._cur = 0
+            self._damp = False  # prev slots already hold the damped field
+            self._sa_raw = torch.zeros(3 * n, **f32) if self._sa_on else None
+        else:
+            self._ab = {
+                "psi_r_A": torch.zeros(psi_n, **f32), "psi_r_prev_A": torch.zeros(psi_n, **f32),
+                "psi_r_B": torch.zeros(psi_n, **f32), "psi_r_prev_B": torch.zeros(psi_n, **f32),
+                "chi_A": torch.full((n,), float(config.chi0), **f32),
+                "chi_prev_A": torch.full((n,), float(config.chi0), **f32),
+                "chi_B": torch.full((n,), float(config.chi0), **f32),
+                "chi_prev_B": torch.full((n,), float(config.chi0), **f32),
+            }
+            if self._has_imag:
+                for k in ("psi_i_A", "psi_i_prev_A", "psi_i_B", "psi_i_prev_B"):
+                    self._ab[k] = torch.zeros(psi_n, **f32)
+            if self._sa_on:
+                self._ab["sa_A"] = torch.zeros(3 * n, **f32)
+                self._ab["sa_B"] = torch.zeros(3 * n, **f32)
+
+    # ------------------------------------------------------------------
+    # buffer attributes of the reference Evolver
+    # ------------------------------------------------------------------
+    def _materialize_prev(self) -> None:
+        """Apply the pending sponge factor to the stored previous Psi (resident mode)."""
+        if self._mode == "resident" and self._damp:
+            p = 1 - self._cur
+            self._pr[p].mul_(self._absorb_psi)
+            if self._has_imag:
+                self._pi[p].mul_(self._absorb_psi)
+            self._damp = False
+
+    def _buf(self, name: str):
+        if self._mode == "ab":
+            return self._ab.get(name)
+        cur, prv = self._cur, 1 - self._cur
+        base = name[:-2]
+        if base == "psi_r":
+            return self._pr[cur]
+        if base == "psi_i":
+            return self._pi[cur]
+        if base == "chi":
+            return self._chi[cur]
+        if base == "chi_prev":
+            return self._chi[prv]
+        if base in ("psi_r_prev", "psi_i_prev"):
+            self._materialize_prev()
+            return (self._pr if base == "psi_r_prev" else self._pi)[prv]
+        if base == "sa":
+            return self._sa_raw
+        raise AttributeError(name)
+
+    # In resident mode the A and B names both refer to the active slots
+    # (the inactive set of the reference holds values no step reads).
+    psi_r_A = property(lambda s: s._buf("psi_r_A"))
+    psi_r_B = property(lambda s: s._buf("psi_r_B"))
+    psi_r_prev_A = property(lambda s: s._buf("psi_r_prev_A"))
+    psi_r_prev_B = property(lambda s: s._buf("psi_r_prev_B"))
+    psi_i_A = property(lambda s: s._buf("psi_i_A"))
+    psi_i_B = property(lambda s: s._buf("psi_i_B"))
+    psi_i_prev_A = property(lambda s: s._buf("psi_i_prev_A"))
+    psi_i_prev_B = property(lambda s: s._buf("psi_i_prev_B"))
+    chi_A = property(lambda s: s._buf("chi_A"))
+    chi_B = property(lambda s: s._buf("chi_B"))
+    chi_prev_A = property(lambda s: s._buf("chi_prev_A"))
+    chi_prev_B = property(lambda s: s._buf("chi_prev_B"))
+    sa_A = property(lambda s: s._buf("sa_A"))
+    sa_B = property(lambda s: s._buf("sa_B"))
+
+    # ------------------------------------------------------------------
+    # time loop (evolver.py:137-180)
+    # ------------------------------------------------------------------
+    def evolve(self, steps: int, callback=None, freeze_chi: bool = False) -> None:
+        """Run `steps` leapfrog steps; callback(evolver, step) every report_interval."""
+        report = self.config.report_interval
+        frozen = None
+        if freeze_chi:
+            if self._mode == "ab":
+                frozen = [self._ab[k].clone() for k in ("chi_A", "chi_B", "chi_prev_A",
+                                                        "chi_prev_B")]
+            else:
+                frozen = [self._chi[self._cur].clone(), self._chi[1 - self._cur].clone()]
+        for _ in range(int(steps)):
+            self._step()
+            if frozen is not None:
+                if self._mode == "ab":
+                    for k, v in zip(("chi_A", "chi_B", "chi_prev_A", "chi_prev_B"), frozen):
+                        self._ab[k].copy_(v)
+                else:
+                    self._chi[self._cur].copy_(frozen[0])
+                    self._chi[1 - self._cur].copy_(frozen[1])
+            self.step += 1
+            if callback is not None and report > 0 and self.step % report == 0:
+                callback(self, self.step)
+
+    def _step(self) -> None:
+        if self._mode == "ab":
+            self._step_ab()
+        else:
+            self._step_resident()
+        self._use_buffer_A = not self._use_buffer_A
+
+    def _step_resident(self) -> None:
+        cfg = self.config
+        cur, prv = self._cur, 1 - self._cur
+        stream = _stream_handle(self.device)
+        table = self._table_dev.data_ptr()
+        desc = ctypes.byref(self._desc)
+        damp = 1 if self._damp else 0
+        common = (float(self._dt2), float(cfg.kappa), float(cfg.lambda_self), float(cfg.chi0),
+                  float(cfg.e0_sq))
+        if self._level == FieldLevel.REAL:
+            _lib.call("lfm_leapfrog_real_f32", self._pr[cur].data_ptr(), self._pr[prv].data_ptr(),
+                      self._chi[cur].data_ptr(), self._chi[prv].data_ptr(), table, desc, damp,
+                      self.N, *common, stream)
+        elif self._level == FieldLevel.COMPLEX:
+            _lib.call("lfm_leapfrog_complex_f32", self._pr[cur].data_ptr(),
+                      self._pr[prv].data_ptr(), self._pi[cur].data_ptr(), self._pi[prv].data_ptr(),
+                      self._chi[cur].data_ptr(), self._chi[prv].data_ptr(), table, desc, damp,
+                      self.N, *common, float(cfg.epsilon_w), stream)
+        else:
+            sa = None
+            if self._sa_on:
+                _lib.call("lfm_helmholtz_sa_f32", self.backend.context.handle,
+                          self._pr[cur].data_ptr(), self._pi[cur].data_ptr(),
+                          self._sa_raw.data_ptr(), self.N, float(cfg.sa_gamma), float(cfg.sa_d),
+                          stream)
+                sa = self._sa_raw.data_ptr()
+            _lib.call("lfm_leapfrog_color_f32", self._pr[cur].data_ptr(), self._pr[prv].data_ptr(),
+                      self._pi[cur].data_ptr(), self._pi[prv].data_ptr(),
+                      self._chi[cur].data_ptr(), self._chi[prv].data_ptr(), table, desc, damp,
+                      self.N, *common, float(cfg.epsilon_w), float(cfg.kappa_c),
+                      float(cfg.epsilon_cc), float(cfg.kappa_string), float(cfg.kappa_tube), sa,
+                      stream)
+        self._cur = prv
+        self._damp = True
+
+    def _step_ab(self) -> None:
+        cfg = self.config
+        b = self._ab
+        src, dst = ("A", "B") if self._use_buffer_A else ("B", "A")
+        g = lambda k, s: b.get(f"{k}_{s}")  # noqa: E731
+        be = self.backend
+        if self._level == FieldLevel.REAL:
+            be.step_real(g("psi_r", src), g("psi_r_prev", src), g("chi", src), g("chi_prev", src),
+                         self.boundary_mask, g("psi_r", dst), g("psi_r_prev", dst), g("chi", dst),
+                         g("chi_prev", dst), self.N, self._dt2, cfg.kappa, cfg.lambda_self,
+                         cfg.chi0, cfg.e0_sq)
+        elif self._level == FieldLevel.COMPLEX:
+            be.step_complex(g("psi_r", src), g("psi_r_prev", src), g("psi_i", src),
+                            g("psi_i_prev", src), g("chi", src), g("chi_prev", src),
+                            self.boundary_mask, g("psi_r", dst), g("psi_r_prev", dst),
+                            g("psi_i", dst), g("psi_i_prev", dst), g("chi", dst),
+                            g("chi_prev", dst), self.N, self._dt2, cfg.kappa, cfg.lambda_self,
+                            cfg.chi0, cfg.e0_sq, cfg.epsilon_w)
+        else:
+            be.step_color(g("psi_r", src), g("psi_r_prev", src), g("psi_i", src),
+                          g("psi_i_prev", src), g("chi", src), g("chi_prev", src),
+                          self.boundary_mask, g("psi_r", dst), g("psi_r_prev", dst),
+                          g("psi_i", dst), g("psi_i_prev", dst), g("chi", dst),
+                          g("chi_prev", dst), self.N, self._dt2, cfg.kappa, cfg.lambda_self,
+                          cfg.chi0, cfg.e0_sq, cfg.epsilon_w, cfg.kappa_c, cfg.epsilon_cc,
+                          kappa_string=cfg.kappa_string, kappa_tube=cfg.kappa_tube,
+                          sa_fields_in=g("sa", src), sa_fields_out=g("sa", dst),
+                          sa_gamma=cfg.sa_gamma, sa_d=cfg.sa_d, dt=cfg.dt)
+
+    # ------------------------------------------------------------------
+    # device views of the active state (no host copies)
+    # ------------------------------------------------------------------
+    def _active(self, field: str):
+        s = "A" if self._use_buffer_A else "B"
+        return getattr(self, f"{field}_{s}")
+
+    def _prev_psi_view(self, imag: bool):
+        """Previous Psi with the sponge factor applied, as the reference stores it."""
+        if self._mode == "ab":
+            return self._active("psi_i_prev" if imag else "psi_r_prev")
+        buf = (self._pi if imag else self._pr)[1 - self._cur]
+        return buf * self._absorb_psi if self._damp else buf
+
+    def _shape(self, flat):
+        if self._level == FieldLevel.COLOR:
+            return flat.reshape(3, self.N, self.N, self.N)
+        return flat.reshape(self.N, self.N, self.N)
+
+    def device_state(self) -> dict:
+        """Device tensors of the current state: psi_r, psi_i, chi, psi_r_prev, psi_i_prev."""
+        out = {"psi_r": self._shape(self._active("psi_r")),
+               "chi": self._active("chi").reshape(self.N, self.N, self.N),
+               "psi_r_prev": self._shape(self._prev_psi_view(False))}
+        if self._has_imag:
+            out["psi_i"] = self._shape(self._active("psi_i"))
+            out["psi_i_prev"] = self._shape(self._prev_psi_view(True))
+        return out
+
+    # ------------------------------------------------------------------
+    # host accessors (evolver.py:289-536)
+    # ------------------------------------------------------------------
+    def _to_host(self, t) -> np.ndarray:
+        return t.detach().to("cpu").numpy()
+
+    def _current_buf(self) -> str:
+        return "A" if self._use_buffer_A else "B"
+
+    def get_chi(self) -> np.ndarray:
+        return self._to_host(self._active("chi")).reshape(self.N, self.N, self.N)
+
+    def get_psi_real(self) -> np.ndarray:
+        return self._shape(self._to_host(self._active("psi_r")))
+
+    def get_psi_imag(self):
+        if not self._has_imag:
+            return None
+        return self._shape(self._to_host(self._active("psi_i")))
+
+    def get_psi_real_prev(self) -> np.ndarray:
+        return self._shape(self._to_host(self._prev_psi_view(False)))
+
+    def get_psi_imag_prev(self):
+        if not self._has_imag:
+            return None
+        return self._shape(self._to_host(self._prev_psi_view(True)))
+
+    def get_energy_density(self) -> np.ndarray:
+        pr = self.get_psi_real()
+        e2 = np.sum(pr**2, axis=0) if pr.ndim == 4 else pr**2
+        pi = self.get_psi_imag()
+        if pi is not None:
+            e2 += np.sum(pi**2, axis=0) if pi.ndim == 4 else pi**2
+        return e2
+
+    def _dev(self, arr):
+        import torch
+
+        return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32).ravel()).to(self.device)
+
+    def _write(self, names, data) -> None:
+        seen = set()
+        for nm in names:
+            buf = getattr(self, nm)
+            if buf is None or id(buf) in seen:
+                continue
+            seen.add(id(buf))
+            if buf.numel() != data.numel():
+                raise ValueError(f"{nm}: got {data.numel()} values, expected {buf.numel()}")
+            buf.copy_(data)
+
+    def set_psi_real(self, arr) -> None:
+        """Set Psi_real current and previous on both buffer sets."""
+        self._write(("psi_r_A", "psi_r_B", "psi_r_prev_A", "psi_r_prev_B"), self._dev(arr))
+
+    def set_psi_imag(self, arr) -> None:
+        if not self._has_imag:
+            raise ValueError("Cannot set imaginary part for REAL field level")
+        self._write(("psi_i_A", "psi_i_B", "psi_i_prev_A", "psi_i_prev_B"), self._dev(arr))
+
+    def set_psi_real_prev(self, arr) -> None:
+        self._write(("psi_r_prev_A", "psi_r_prev_B"), self._dev(arr))
+
+    def set_psi_imag_prev(self, arr) -> None:
+        if not self._has_imag:
+            raise ValueError("Cannot set imaginary part for REAL field level")
+        self._write(("psi_i_prev_A", "psi_i_prev_B"), self._dev(arr))
+
+    def set_psi_real_current(self, arr) -> None:
+        self._active("psi_r").copy_(self._dev(arr))
+
+    def set_psi_imag_current(self, arr) -> None:
+        if not self._has_imag:
+            raise ValueError("Cannot set imaginary part for REAL field level")
+        self._active("psi_i").copy_(self._dev(arr))
+
+    def set_chi(self, arr) -> None:
+        self._write(("chi_A", "chi_B", "chi_prev_A", "chi_prev_B"), self._dev(arr))
+
+    def set_chi_current(self, arr) -> None:
+        self._write(("chi_A", "chi_B"), self._dev(arr))
+
+    def set_chi_prev(self, arr) -> None:
+        self._write(("chi_prev_A", "chi_prev_B"), self._dev(arr))
+
+    def get_sa_fields(self):
+        """S_a fields (3, N, N, N) as last computed, clipped at 0; None when off."""
+        if not self._sa_on:
+            return None
+        buf = self._active("sa") if self._mode == "ab" else self._sa_raw
+        return self._to_host(buf.clamp_min(0.0)).reshape(3, self.N, self.N, self.N)
+
+    def set_sa_fields(self, arr) -> None:
+        if not self._sa_on:
+            raise ValueError(
+                "SA fields not allocated — set kappa_tube > 0 in SimulationConfig"
+                " before creating the Evolver."
+            )
+        data = self._dev(arr)
+        if self._mode == "ab":
+            self._ab["sa_A"].copy_(data)
+            self._ab["sa_B"].copy_(data)
+        else:
+            self._sa_raw.copy_(data)

@@ -1,0 +1,136 @@
+"""C ABI checks that need no GPU: the library builds, loads, exports every
+function include/lfm_b200.h declares, and its host-side mask table is exact."""
+
+from __future__ import annotations
+
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from lfm_b200 import _lib
+    from lfm_b200.build import build_library
+
+    build_library()
+    return _lib.load()
+
+
+def header_functions() -> list[str]:
+    text = (ROOT / "include" / "lfm_b200.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+char\*|int)\s+(lfm_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_the_abi():
+    names = header_functions()
+    for must in ("lfm_step_real_f32", "lfm_step_complex_f32", "lfm_step_color_f32",
+                 "lfm_leapfrog_real_f32", "lfm_helmholtz_sa_f32", "lfm_mask_lut_build"):
+        assert must in names
+
+
+def test_library_exports_every_declared_function(lib):
+    from lfm_b200 import _lib
+
+    missing = [n for n in header_functions() if not hasattr(lib, n)]
+    assert not missing, f"not exported: {missing}"
+    # the Python binding covers the whole header
+    assert set(header_functions()) <= set(_lib.exported_symbols())
+    assert lib.lfm_abi_version() == 1
+
+
+def test_strerror_names_codes(lib):
+    assert lib.lfm_strerror(0) == b"ok"
+    assert lib.lfm_strerror(6).startswith(b"mask")
+
+
+@pytest.mark.parametrize("N", [8, 12, 13, 16, 33, 64, 96])
+@pytest.mark.parametrize("bf", [0.15, 0.3, 0.5])
+def test_mask_table_reproduces_mask_exactly(lib, N, bf):
+    from lfm_b200.mask import MaskTable, boundary_mask, radial_keys
+
+    m = boundary_mask(N, bf)
+    t = MaskTable.from_mask(N, m)
+    assert t.desc.shift == (3 if N % 2 == 0 else 2)
+    got = t.lookup(radial_keys(N))
+    assert np.array_equal(got.view(np.uint32), m.view(np.uint32))
+    # the table is small: the sponge band only
+    assert t.table.size <= (3 * N * N) // 4 + 16
+
+
+def test_mask_matches_reference_fixture(lib):
+    from lfm_b200.mask import boundary_mask
+
+    g = load_golden("masks.npz")
+    for key, ref in g.items():
+        if key.startswith("mask_"):
+            _, N, bf = key.split("_")
+            assert np.array_equal(boundary_mask(int(N), float(bf)), ref), key
+
+
+def test_mask_table_rejects_non_radial_mask(lib):
+    from lfm_b200._lib import LFM_ERR_MASK, LfmError
+    from lfm_b200.mask import MaskTable, boundary_mask
+
+    m = boundary_mask(16, 0.3).copy()
+    band = np.flatnonzero((m > 0) & (m < 1))
+    m[band[0]] = 0.123  # break radial symmetry
+    with pytest.raises(LfmError) as e:
+        MaskTable.from_mask(16, m)
+    assert e.value.code == LFM_ERR_MASK
+
+
+def test_mask_table_edge_cases(lib):
+    from lfm_b200.mask import MaskTable, radial_keys
+
+    N = 10
+    zero = MaskTable.from_mask(N, np.zeros(N**3, np.float32))
+    assert (zero.lookup(radial_keys(N)) == 0).all()
+    one = MaskTable.from_mask(N, np.ones(N**3, np.float32))
+    assert (one.lookup(radial_keys(N)) == 1).all()
+
+
+def test_bad_sizes_are_rejected(lib):
+    import ctypes
+
+    from lfm_b200._lib import LFM_ERR_CAPACITY, LFM_ERR_INVALID_ARG, LfmError, MaskLut, call
+    from lfm_b200.mask import boundary_mask
+
+    d = MaskLut()
+    with pytest.raises(LfmError) as e:
+        call("lfm_mask_lut_build", 1, None, None, 0, ctypes.byref(d))
+    assert e.value.code == LFM_ERR_INVALID_ARG
+    m = boundary_mask(16, 0.3)
+    tiny = np.zeros(2, np.float32)
+    with pytest.raises(LfmError) as e:
+        call("lfm_mask_lut_build", 16, m.ctypes.data, tiny.ctypes.data, 2, ctypes.byref(d))
+    assert e.value.code == LFM_ERR_CAPACITY
+    with pytest.raises(LfmError) as e:
+        call("lfm_step_real_f32", *([None] * 9), 16, 4e-4, 1 / 63, 0.0, 19.0, 0.0, None)
+    assert e.value.code == LFM_ERR_INVALID_ARG
+
+
+def test_config_validation_matches_reference_rules():
+    from lfm_b200.config import FieldLevel, SimulationConfig, full_physics, gravity_only
+
+    with pytest.raises(ValueError, match="grid_size"):
+        SimulationConfig(grid_size=4)
+    with pytest.raises(ValueError, match="CFL"):
+        SimulationConfig(dt=0.06)
+    with pytest.raises(ValueError, match="boundary_fraction"):
+        SimulationConfig(boundary_fraction=1.0)
+    c = gravity_only(64)
+    assert c.field_level == FieldLevel.REAL and c.kappa == pytest.approx(1 / 63)
+    f = full_physics(32)
+    assert f.sa_enabled and f.lambda_self == pytest.approx(4 / 31)
+    assert f.kappa_tube == pytest.approx(30 / 63) and f.sa_d == pytest.approx(4.9)
+
+
+def test_product_does_not_import_the_oracle():
+    pkg = ROOT / "lfm-physics_b200"
+    for p in list(pkg.rglob("*.py")) + list(pkg.rglob("*.cu")) + list(pkg.rglob("*.cuh")):
+        text = p.read_text()
+        assert not re.search(r"(from|import)\s+oracle|lfm_oracle|oracle/", text), p
