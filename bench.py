@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Benchmark of the fused leapfrog step: REAL level, 512^3 lattice, float32.
+
+One "step" is one leapfrog step (GOV-01 + GOV-02 over the 19-point
+Laplacian, sponge, clamp) of the whole lattice.  The workload is the
+throughput configuration: chi = 19 + U(-1e-3, 1e-3), 64 Gaussian packets
+(amplitude U[2,6], sigma U[2,4]) inside the sponge-free sphere, E_prev = E;
+synthetic, seeded.  Inputs (4 x 537 MB) are larger than L2, so no flush is
+needed between steps.
+
+Prints one JSON line (rank 0).  `value` is device-timed (CUDA events around
+K steps on the launching stream, max over ranks) with the state resident in
+HBM; `e2e` is the same metric through the public API (Evolver) with the
+initial state copied from pinned host memory and the final fields copied
+back inside the timed region.  --impl reference times the CPU oracle (the
+bit-exact restatement of the reference NumPy path) on the host cores.
+
+Multi-GPU (torchrun): every rank evolves its own lattice (independent
+lattices, no collective in the data path): weak scaling.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "lfm-physics_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+BYTES_PER_CELL = {"real": 24}          # algorithmic: read E, E_prev, chi, chi_prev; write E', chi'
+METRIC = "GCell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--N", type=int, default=512)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="approximate CPU time of the oracle baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:  # noqa: BLE001
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(N: int):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        e = d.get(f"real_{N}")
+        return None if e is None else float(e["dram_bytes_per_launch"])
+    except Exception:  # noqa: BLE001
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait(timeout=5)
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = max((num(r[2]) for r in rows if num(r[2])), default=None)
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        sm_sorted = sorted(sm)
+        med = sm_sorted[len(sm_sorted) // 2] if sm_sorted else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(N: int, seconds: float, E, chi) -> dict:
+    """The oracle (bit-exact restatement of the reference CPU path), all host threads,
+    on slabs of the same lattice until about `seconds` of work."""
+    import numpy as np
+
+    from lfm_b200.config import gravity_only
+    from lfm_b200.mask import boundary_mask
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    cfg = gravity_only(N)
+    n = N**3
+    Ef = E.reshape(-1)
+    chif = chi.reshape(-1)
+    mask = boundary_mask(N, cfg.boundary_fraction)  # same bits as the reference mask
+    outs = [np.empty(n, np.float32) for _ in range(4)]
+    be = O.OracleBackend()
+    planes = min(N, max(threads, 16))
+    done_cells = 0
+    t0 = time.perf_counter()
+    i0 = 0
+    while True:
+        O.set_plane_range(i0, i0 + planes)
+        be.step_real(Ef, Ef, chif, chif, mask, *outs, N, cfg.dt**2, cfg.kappa, cfg.lambda_self,
+                     cfg.chi0, cfg.e0_sq)
+        done_cells += planes * N * N
+        i0 = (i0 + planes) % N
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    O.set_plane_range(0, -1)
+    return {"value": done_cells / el / 1e9, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"oracle REAL step on {done_cells // (N * N)} planes of the {N}^3 lattice "
+                      f"({el:.1f} s, {threads} threads of {os.cpu_count()})"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    from lfm_b200.config import gravity_only
+    from lfm_b200.mask import boundary_mask
+    from lfm_b200.workloads import real_solitons
+    from oracle import oracle as O
+
+    N = args.N
+    E, chi = real_solitons(N)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    cfg = gravity_only(N)
+    n = N**3
+    bufs = [E.reshape(-1).copy(), E.reshape(-1).copy(), chi.reshape(-1).copy(),
+            chi.reshape(-1).copy()]
+    outs = [np.empty(n, np.float32) for _ in range(4)]
+    mask = boundary_mask(N, cfg.boundary_fraction)
+    be = O.OracleBackend()
+    planes = min(N, threads)
+
+    def step(i0):
+        O.set_plane_range(i0, i0 + planes)
+        be.step_real(*bufs, mask, *outs, N, cfg.dt**2, cfg.kappa, cfg.lambda_self, cfg.chi0,
+                     cfg.e0_sq)
+
+    # Each reference "step" is a slab of the lattice, sized from a calibration
+    # step so that warm-up plus timed steps take about a minute of host time.
+    t0 = time.perf_counter()
+    step(0)
+    rate = planes * N * N / max(time.perf_counter() - t0, 1e-6)
+    budget = 60.0 / max(args.steps + args.warmup, 1)
+    planes = int(max(1, min(N, rate * budget // (N * N))))
+
+    for w in range(args.warmup):
+        step((w * planes) % N)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        step((s * planes) % N)
+    el = time.perf_counter() - t0
+    O.set_plane_range(0, -1)
+    cells = planes * N * N * args.steps
+    value = cells / el / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"REAL {N}^3 leapfrog step, 64 packets", "N": N,
+                   "level": "REAL", "sample_planes_per_step": planes},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{planes} planes of the {N}^3 lattice per step"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from lfm_b200 import B200Backend, Evolver, _lib
+    from lfm_b200.config import gravity_only
+    from lfm_b200.workloads import real_solitons
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    N = args.N
+    E, chi = real_solitons(N, seed_chi=1 + 1000 * rank, seed_solitons=2 + 1000 * rank)
+    be = B200Backend(dev)
+    ev = Evolver(gravity_only(N), backend=be)
+    ev.set_psi_real(E)
+    ev.set_chi(chi)
+    ev.evolve(max(args.warmup, 3))
+    ev.warm_graphs()
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-timed, state resident in HBM -------------------------------
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    ev.evolve(args.steps)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clock_info = clocks.stop()
+    ms = max_over_ranks(t_start.elapsed_time(t_end))
+    status = _lib.device_status(clear=True)
+    if status:
+        raise RuntimeError(f"device status word {status} after the timed steps")
+    cells = N**3
+    value = world * cells * args.steps / (ms / 1e3) / 1e9
+    ms_per_step = ms / args.steps
+    cfg_used = _lib.tune_get(0, N)
+
+    peak, peak_kind = measured_peaks()
+    bytes_per_launch = BYTES_PER_CELL["real"] * cells
+    achieved = bytes_per_launch / (ms_per_step / 1e3) / 1e9
+
+    # ---- end to end through the public API ---------------------------------
+    e2e = None
+    if not args.no_e2e:
+        E_h = torch.from_numpy(E).pin_memory()
+        chi_h = torch.from_numpy(chi).pin_memory()
+        chi_out = torch.empty_like(chi_h).pin_memory()
+        E_out = torch.empty_like(E_h).pin_memory()
+        ev2 = Evolver(gravity_only(N), backend=be)
+        ev2.set_psi_real(E_h)
+        ev2.set_chi(chi_h)
+        ev2.evolve(4)
+        ev2.warm_graphs()  # capture both step graphs outside the timed region
+        torch.cuda.synchronize(dev)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ev2.set_psi_real(E_h)
+        ev2.set_chi(chi_h)
+        ev2.evolve(args.steps)
+        ev2.get_chi(out=chi_out)
+        ev2.get_psi_real(out=E_out)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ms2 = max_over_ranks(a.elapsed_time(b))
+        h2d = E_h.numel() * 4 + chi_h.numel() * 4
+        d2h = chi_out.numel() * 4 + E_out.numel() * 4
+        e2e = {"value": world * cells * args.steps / (ms2 / 1e3) / 1e9, "unit": METRIC,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "job": f"set_psi_real + set_chi from pinned host, evolve({args.steps}), "
+                      "get_chi + get_psi_real to pinned host",
+               "ms": ms2}
+        if not np.isfinite(chi_out.numpy()).all():
+            raise RuntimeError("non-finite chi after the end-to-end run")
+        del ev2
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"REAL {N}^3 leapfrog step (GOV-01 + GOV-02, 19-point, sponge), "
+                               "64 packets, chi0 = 19 +- 1e-3",
+                   "N": N, "level": "REAL", "buffers": "resident", "bytes_per_cell": 24,
+                   "l2": "inputs 2.1 GB > L2, no flush", "parallelism": f"independent lattices x{world}",
+                   "tile": cfg_used},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": profiled_traffic(N),
+                     "algorithmic_bytes_per_launch": bytes_per_launch},
+        "clocks": clock_info,
+        "gpu_launches": args.steps,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -20,6 +20,8 @@
 // Every mbarrier wait is bounded by wall time (%globaltimer); on timeout the
 // CTA records LFM_ERR_DEVICE_TIMEOUT in the status word, waits (bounded)
 // for its own copies in flight and returns.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -467,7 +469,9 @@ struct Choice {
   int TJ = 0, S = 0, IC = 0, threads = 0, smem = 0;
 };
 
-constexpr int kSmemLimit = 227 * 1024;
+// Dynamic shared memory a configuration may use: the 227 KB opt-in limit
+// less 1 KB for the kernel's static shared memory (mbarriers, abort flag).
+constexpr int kSmemLimit = 226 * 1024;
 
 int stage_bytes(int N, int TJ, int ns, int np) { return 4 * N * (ns * (TJ + 2) + np * TJ); }
 
@@ -507,23 +511,47 @@ Choice choose(int level, int N, int V, int ns, int np) {
   if (have_forced && forced.ic > 0) {
     best.IC = std::min(forced.ic, N);
   } else {
-    // about four waves of tiles over 148 SMs, at least 8 planes per chunk
-    const long target_tiles = 4L * 148 * ctas;
-    int ic = (int)(((long)N * JT + target_tiles - 1) / target_tiles);
-    best.IC = std::max(8, std::min(ic, N));
+    // Planes per chunk: balance the last wave of tiles over 148 SMs against
+    // the two halo planes each chunk loads in addition to its own.
+    const double slots = 148.0 * ctas;
+    double best_eff = -1.0;
+    for (int ic = std::min(8, N); ic <= N; ++ic) {
+      const int chunks = (N + ic - 1) / ic;
+      const double waves = (double)JT * chunks / slots;
+      const double fill = waves / std::ceil(waves);
+      const double eff = fill * (double)N / (N + 2.0 * chunks);
+      if (eff > best_eff + 1e-9) {
+        best_eff = eff;
+        best.IC = ic;
+      }
+    }
   }
   return best;
 }
 
 template <int LEVEL, int V>
 cudaError_t launch_level(const TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  static std::once_flag once;
-  static cudaError_t attr_err = cudaSuccess;
-  std::call_once(once, [] {
-    attr_err = cudaFuncSetAttribute(tma_step_kernel<LEVEL, V>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit);
-  });
-  if (attr_err != cudaSuccess) return attr_err;
+  // Raise the kernel's dynamic shared-memory limit to what this launch needs,
+  // within the device's opt-in limit less the kernel's static shared memory.
+  static std::mutex mu;
+  static int granted = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (ch.smem > granted) {
+      int dev = 0, optin = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      cudaFuncAttributes fa{};
+      if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, tma_step_kernel<LEVEL, V>);
+      if (e != cudaSuccess) return e;
+      if (ch.smem + (int)fa.sharedSizeBytes > optin) return cudaErrorNotSupported;
+      e = cudaFuncSetAttribute(tma_step_kernel<LEVEL, V>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, ch.smem);
+      if (e != cudaSuccess) return e;
+      granted = ch.smem;
+    }
+  }
   const int JT = P.N / P.TJ;
   const int chunks = (P.N + P.IC - 1) / P.IC;
   tma_step_kernel<LEVEL, V><<<JT * chunks, ch.threads, ch.smem, stream>>>(P);

@@ -58,6 +58,8 @@ _SIGNATURES = {
     "lfm_helmholtz_sa_f32": [_P] * 4 + [c_int, _D, _D, _P],
     "lfm_sa_clip_f32": [_P, _P, c_int64, _P],
     "lfm_device_status": [POINTER(c_int), c_int],
+    "lfm_tune_set": [c_int] * 5,
+    "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 5,
 }
 
 _lib = None
@@ -104,6 +106,20 @@ def call(name: str, *args) -> None:
 def set_step_path(path: int) -> None:
     """Choose the step kernel: 0 automatic, 1 direct, 2 fused 2.5D only."""
     call("lfm_set_step_path", int(path))
+
+
+def tune_set(level: int, N: int, tj: int, stages: int, ic: int = 0) -> None:
+    """Force the fused kernel's tile configuration for (level, N); tj <= 0 clears it."""
+    call("lfm_tune_set", int(level), int(N), int(tj), int(stages), int(ic))
+
+
+def tune_get(level: int, N: int) -> dict | None:
+    """The tile configuration the last fused step of (level, N) used, or None."""
+    vals = [c_int(0) for _ in range(5)]
+    rc = load().lfm_tune_get(int(level), int(N), *[ctypes.byref(v) for v in vals])
+    if rc != LFM_OK:
+        return None
+    return dict(zip(("tj", "stages", "ic", "threads", "smem"), (v.value for v in vals)))
 
 
 def device_status(clear: bool = True) -> int:

@@ -33,7 +33,7 @@ import numpy as np
 from . import _lib
 from .backend import B200Backend, _stream_handle, get_backend
 from .config import FieldLevel
-from .mask import MaskTable, boundary_mask as host_boundary_mask
+from .mask import MaskTable
 
 
 class Evolver:
@@ -67,8 +67,8 @@ class Evolver:
         N, n = self.N, self.total
         psi_n = self._n_psi * n
         f32 = dict(dtype=torch.float32, device=self.device)
-        mask_np = host_boundary_mask(N, config.boundary_fraction)
-        self.boundary_mask = torch.from_numpy(mask_np).to(self.device)
+        self._table = MaskTable.for_lattice(N, config.boundary_fraction)
+        self.boundary_mask = self._table.device_mask(self.device)
         self._absorb = 1.0 - self.boundary_mask  # float32, as numpy_backend.py:122
         if self._level == FieldLevel.COLOR:
             self._absorb_psi = self._absorb.repeat(3)
@@ -76,7 +76,6 @@ class Evolver:
             self._absorb_psi = self._absorb
 
         if self._mode == "resident":
-            self._table = MaskTable.from_mask(N, mask_np)
             self._table_dev = self._table.to_device(self.device)
             self._desc = self._table.desc
             self._pr = [torch.zeros(psi_n, **f32), torch.zeros(psi_n, **f32)]
@@ -154,9 +153,16 @@ class Evolver:
     # ------------------------------------------------------------------
     # time loop (evolver.py:137-180)
     # ------------------------------------------------------------------
+    use_graphs = True
+    """Replay captured CUDA graphs of two steps when evolve() has no per-step host work."""
+
     def evolve(self, steps: int, callback=None, freeze_chi: bool = False) -> None:
         """Run `steps` leapfrog steps; callback(evolver, step) every report_interval."""
         report = self.config.report_interval
+        if (callback is None and not freeze_chi and self._mode == "resident"
+                and self.use_graphs and steps >= 4):
+            self._evolve_graphed(int(steps))
+            return
         frozen = None
         if freeze_chi:
             if self._mode == "ab":
@@ -176,6 +182,59 @@ class Evolver:
             self.step += 1
             if callback is not None and report > 0 and self.step % report == 0:
                 callback(self, self.step)
+
+    def _param_key(self) -> tuple:
+        c = self.config
+        return (self._cur, float(c.dt), float(c.kappa), float(c.lambda_self), float(c.chi0),
+                float(c.e0_sq), float(c.epsilon_w), float(c.kappa_c), float(c.epsilon_cc),
+                float(c.kappa_string), float(c.kappa_tube), float(c.sa_gamma), float(c.sa_d))
+
+    def _pair_graph(self):
+        """CUDA graph of two resident steps from the current slot parity."""
+        import torch
+
+        if not hasattr(self, "_graphs"):
+            self._graphs = {}
+        key = self._param_key()
+        g = self._graphs.get(key)
+        if g is None:
+            saved = (self._cur, self._damp, self._use_buffer_A)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._step_resident()
+                self._step_resident()
+            self._cur, self._damp, self._use_buffer_A = saved
+            self._graphs[key] = g
+        return g
+
+    def warm_graphs(self) -> None:
+        """Capture the two-step graphs of both slot parities now (nothing runs), so a
+        later evolve() does not capture inside a timed region.  Needs one step done."""
+        if self._mode != "resident" or not self._damp:
+            return
+        saved = self._cur
+        for c in (0, 1):
+            self._cur = c
+            self._pair_graph()
+        self._cur = saved
+
+    def _evolve_graphed(self, steps: int) -> None:
+        self._dt2 = self.config.dt**2
+        done = 0
+        if not self._damp:
+            # first step after a host write: the kernel must not damp prev
+            self._step()
+            self.step += 1
+            done = 1
+        pairs = (steps - done) // 2
+        if pairs:
+            g = self._pair_graph()
+            for _ in range(pairs):
+                g.replay()
+            self.step += 2 * pairs
+        if (steps - done) % 2:
+            self._step()
+            self.step += 1
 
     def _step(self) -> None:
         if self._mode == "ab":
@@ -280,16 +339,26 @@ class Evolver:
     # ------------------------------------------------------------------
     # host accessors (evolver.py:289-536)
     # ------------------------------------------------------------------
-    def _to_host(self, t) -> np.ndarray:
+    def _to_host(self, t, out=None):
+        """Host copy of a device tensor; into `out` (e.g. pinned) without a sync when given."""
+        if out is not None:
+            out.reshape(-1).copy_(t.reshape(-1), non_blocking=True)
+            return out
         return t.detach().to("cpu").numpy()
 
     def _current_buf(self) -> str:
         return "A" if self._use_buffer_A else "B"
 
-    def get_chi(self) -> np.ndarray:
+    def get_chi(self, out=None):
+        """Current chi, (N, N, N).  With `out` (a host tensor, e.g. pinned) the copy
+        is asynchronous on the current stream and `out` is returned."""
+        if out is not None:
+            return self._to_host(self._active("chi"), out)
         return self._to_host(self._active("chi")).reshape(self.N, self.N, self.N)
 
-    def get_psi_real(self) -> np.ndarray:
+    def get_psi_real(self, out=None):
+        if out is not None:
+            return self._to_host(self._active("psi_r"), out)
         return self._shape(self._to_host(self._active("psi_r")))
 
     def get_psi_imag(self):
@@ -314,11 +383,17 @@ class Evolver:
         return e2
 
     def _dev(self, arr):
+        """Flat float32 view of a host array or tensor (copied to the device by _write)."""
         import torch
 
-        return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32).ravel()).to(self.device)
+        if isinstance(arr, torch.Tensor):
+            return arr.detach().reshape(-1).to(dtype=torch.float32)
+        return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32).ravel())
 
     def _write(self, names, data) -> None:
+        """Copy `data` (host or device) into the named buffers: one host->device
+        copy (asynchronous from pinned memory), device->device for the rest."""
+        first = None
         seen = set()
         for nm in names:
             buf = getattr(self, nm)
@@ -327,7 +402,11 @@ class Evolver:
             seen.add(id(buf))
             if buf.numel() != data.numel():
                 raise ValueError(f"{nm}: got {data.numel()} values, expected {buf.numel()}")
-            buf.copy_(data)
+            if first is None:
+                buf.copy_(data, non_blocking=True)
+                first = buf
+            else:
+                buf.copy_(first)
 
     def set_psi_real(self, arr) -> None:
         """Set Psi_real current and previous on both buffer sets."""
@@ -347,12 +426,12 @@ class Evolver:
         self._write(("psi_i_prev_A", "psi_i_prev_B"), self._dev(arr))
 
     def set_psi_real_current(self, arr) -> None:
-        self._active("psi_r").copy_(self._dev(arr))
+        self._active("psi_r").copy_(self._dev(arr), non_blocking=True)
 
     def set_psi_imag_current(self, arr) -> None:
         if not self._has_imag:
             raise ValueError("Cannot set imaginary part for REAL field level")
-        self._active("psi_i").copy_(self._dev(arr))
+        self._active("psi_i").copy_(self._dev(arr), non_blocking=True)
 
     def set_chi(self, arr) -> None:
         self._write(("chi_A", "chi_B", "chi_prev_A", "chi_prev_B"), self._dev(arr))

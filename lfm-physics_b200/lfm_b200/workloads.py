@@ -1,0 +1,92 @@
+"""Seeded synthetic initial states of the benchmark workloads.
+
+The reference measures on synthetic lattices only; these builders produce
+states with the shapes, sizes and value distributions of the five workloads
+the benchmark and the parity tests use.  Gaussian packets follow
+amplitude*exp(-r^2/(2 sigma^2)) as lfm/fields/soliton.py:49-59 builds them,
+evaluated on a box of +-6 sigma around each centre (the envelope is below
+2e-8 of its peak outside it) so that 512^3 states build in seconds.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def add_gaussian(field: np.ndarray, center, amplitude: float, sigma: float,
+                 phase_factor: complex | float = 1.0) -> None:
+    """Accumulate amplitude*exp(-r^2/(2 sigma^2)) (times phase_factor) into a float64 field."""
+    N = field.shape[-1]
+    reach = int(math.ceil(6.0 * sigma))
+    idx = []
+    for c in center:
+        lo = int(math.floor(c)) - reach
+        idx.append(np.arange(lo, lo + 2 * reach + 2))
+    dx = [(ix - c) ** 2 for ix, c in zip(idx, center)]
+    r2 = dx[0][:, None, None] + dx[1][None, :, None] + dx[2][None, None, :]
+    env = amplitude * np.exp(-r2 / (2.0 * sigma * sigma))
+    sel = np.ix_(*(ix % N for ix in idx))
+    if 2 * reach + 2 <= N:
+        field[sel] += env * phase_factor  # no index repeats inside the box
+    else:
+        np.add.at(field, sel, env * phase_factor)
+
+
+def real_solitons(N: int, count: int = 64, seed_chi: int = 1, seed_solitons: int = 2):
+    """Throughput state at the REAL level (the 512^3 benchmark workload).
+
+    chi = 19 + U(-1e-3, 1e-3) (seed_chi); `count` packets with amplitude
+    U[2, 6] and sigma U[2, 4] cells, centred uniformly inside the sponge-free
+    sphere |x - N/2| < 0.35 N - 3 sigma (seed_solitons).  Returns float32
+    (E, chi), each (N, N, N); E_prev = E.
+    """
+    rng_c = np.random.default_rng(seed_chi)
+    chi = (19.0 + rng_c.uniform(-1e-3, 1e-3, size=(N, N, N))).astype(np.float32)
+    rng = np.random.default_rng(seed_solitons)
+    E = np.zeros((N, N, N), dtype=np.float64)
+    c0 = N / 2.0
+    for _ in range(count):
+        amp = rng.uniform(2.0, 6.0)
+        sigma = rng.uniform(2.0, 4.0)
+        rmax = 0.35 * N - 3.0 * sigma
+        while True:
+            p = rng.uniform(c0 - rmax, c0 + rmax, size=3)
+            if np.sum((p - c0) ** 2) < rmax * rmax:
+                break
+        add_gaussian(E, tuple(p), amp, sigma)
+    return E.astype(np.float32), chi
+
+
+def config1_soliton(N: int = 64, seed: int = 42):
+    """REAL 64^3 parity workload: packet (6.0, sigma 3) at the centre + 1e-4 N(0,1) noise."""
+    x = np.arange(N, dtype=np.float32)
+    c = N // 2
+    r2 = ((x - c) ** 2)[:, None, None] + ((x - c) ** 2)[None, :, None] + ((x - c) ** 2)[None, None, :]
+    env = (6.0 * np.exp(-r2 / (2.0 * 3.0**2))).astype(np.float32)
+    rng = np.random.default_rng(seed)
+    return (env + 1e-4 * rng.standard_normal((N,) * 3)).astype(np.float32)
+
+
+def color_packets(N: int = 256, seed_phase: int = 3, seed_chi: int = 4):
+    """COLOR workload: two colour-charged packets (amplitude 4, sigma 3), 40 cells apart.
+
+    Each packet carries a seeded random colour-phase vector theta_a ~ U[0, 2pi):
+    Psi_a = A g(r) e^{i theta_a} / sqrt(3).  chi = 19 +- 1e-3 (seed_chi).
+    Returns float32 (psi_r, psi_i) of shape (3, N, N, N) and chi (N, N, N).
+    """
+    rng = np.random.default_rng(seed_phase)
+    pr = np.zeros((3, N, N, N), dtype=np.float64)
+    pi = np.zeros((3, N, N, N), dtype=np.float64)
+    c = N / 2.0
+    centres = ((c, c - 20.0, c), (c, c + 20.0, c))
+    for ctr in centres:
+        theta = rng.uniform(0.0, 2.0 * np.pi, size=3)
+        for a in range(3):
+            f = np.exp(1j * theta[a]) / np.sqrt(3.0)
+            add_gaussian(pr[a], ctr, 4.0, 3.0, f.real)
+            add_gaussian(pi[a], ctr, 4.0, 3.0, f.imag)
+    rng_c = np.random.default_rng(seed_chi)
+    chi = (19.0 + rng_c.uniform(-1e-3, 1e-3, size=(N, N, N))).astype(np.float32)
+    return pr.astype(np.float32), pi.astype(np.float32), chi

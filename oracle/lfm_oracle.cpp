@@ -33,20 +33,26 @@
 namespace {
 
 int g_threads = 1;
+// Planes [g_i0, g_i1) of the slowest axis are stepped (default: all).  The
+// CPU baseline uses this to time a bounded slab of a large lattice.
+int g_i0 = 0, g_i1 = -1;
 
 // Runs body(i) for i in [0, n) on g_threads std::threads, split into
 // contiguous slabs of the slowest axis.
 template <typename F>
 void parallel_for(int n, F body) {
-  const int t = std::max(1, std::min(g_threads, n));
+  const int a = std::max(0, std::min(g_i0, n));
+  const int b = (g_i1 < 0) ? n : std::max(a, std::min(g_i1, n));
+  const int m = b - a;
+  const int t = std::max(1, std::min(g_threads, m));
   if (t == 1) {
-    for (int i = 0; i < n; ++i) body(i);
+    for (int i = a; i < b; ++i) body(i);
     return;
   }
   std::vector<std::thread> pool;
   pool.reserve(t);
   for (int w = 0; w < t; ++w) {
-    const int lo = (int)((int64_t)n * w / t), hi = (int)((int64_t)n * (w + 1) / t);
+    const int lo = a + (int)((int64_t)m * w / t), hi = a + (int)((int64_t)m * (w + 1) / t);
     pool.emplace_back([=, &body] { for (int i = lo; i < hi; ++i) body(i); });
   }
   for (auto& th : pool) th.join();
@@ -379,6 +385,10 @@ void step_color(const T* Pr, const T* Prp, const T* Pi, const T* Pip, const T* c
 extern "C" {
 
 void oracle_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+void oracle_set_plane_range(int i0, int i1) {
+  g_i0 = i0;
+  g_i1 = i1;
+}
 int oracle_max_threads(void) {
   unsigned h = std::thread::hardware_concurrency();
   return h ? (int)h : 1;

@@ -65,6 +65,7 @@ def _load():
             fn.argtypes = [p, p, ctypes.c_int]
             fn.restype = None
         lib.oracle_set_threads.argtypes = [ctypes.c_int]
+        lib.oracle_set_plane_range.argtypes = [ctypes.c_int, ctypes.c_int]
         lib.oracle_max_threads.restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -72,6 +73,11 @@ def _load():
 
 def set_threads(n: int) -> None:
     _load().oracle_set_threads(int(n))
+
+
+def set_plane_range(i0: int = 0, i1: int = -1) -> None:
+    """Step only planes [i0, i1) of the slowest axis (i1 < 0: to the end)."""
+    _load().oracle_set_plane_range(int(i0), int(i1))
 
 
 def max_threads() -> int:

@@ -62,13 +62,33 @@ def test_mask_table_reproduces_mask_exactly(lib, N, bf):
 
 
 def test_mask_matches_reference_fixture(lib):
-    from lfm_b200.mask import boundary_mask
+    import hashlib
+    import json
+
+    from lfm_b200.mask import MaskTable, boundary_mask, radial_keys
 
     g = load_golden("masks.npz")
     for key, ref in g.items():
         if key.startswith("mask_"):
             _, N, bf = key.split("_")
             assert np.array_equal(boundary_mask(int(N), float(bf)), ref), key
+    for key, h in json.loads(str(g["large_mask_sha256"])).items():
+        N, bf = int(key.split("_")[0]), float(key.split("_")[1])
+        assert hashlib.sha256(boundary_mask(N, bf).tobytes()).hexdigest() == h, key
+        # the formula-built table gives the same bits through the key lookup
+        t = MaskTable.for_lattice(N, bf)
+        assert hashlib.sha256(t.lookup(radial_keys(N)).tobytes()).hexdigest() == h, key
+
+
+@pytest.mark.parametrize("N", [8, 13, 16, 33, 64])
+@pytest.mark.parametrize("bf", [0.15, 0.3, 0.5, 0.9])
+def test_formula_table_equals_scanned_table(lib, N, bf):
+    from lfm_b200.mask import MaskTable, boundary_mask, radial_keys
+
+    a = MaskTable.for_lattice(N, bf)
+    b = MaskTable.from_mask(N, boundary_mask(N, bf))
+    q = radial_keys(N)
+    assert np.array_equal(a.lookup(q).view(np.uint32), b.lookup(q).view(np.uint32))
 
 
 def test_mask_table_rejects_non_radial_mask(lib):

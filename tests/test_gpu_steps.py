@@ -328,6 +328,25 @@ def test_setters_mid_run_keep_reference_semantics(be):
     del rng
 
 
+@pytest.mark.parametrize("level", ["real", "complex", "color"])
+def test_graph_replay_equals_eager_steps(be, level):
+    from lfm_b200 import Evolver
+
+    cfg = _parity_config(level)
+    E = O.parity_seed_blob(16)
+    runs = []
+    for graphs in (True, False):
+        ev = Evolver(cfg, backend=be)
+        ev.use_graphs = graphs
+        _seed(ev, level, E)
+        ev.evolve(37)
+        ev.evolve(12)
+        runs.append((ev.get_psi_real(), ev.get_chi(), ev.get_psi_real_prev(), ev.step))
+    for a, b in zip(runs[0][:3], runs[1][:3]):
+        assert bits_equal(a, b)
+    assert runs[0][3] == runs[1][3] == 49
+
+
 def test_freeze_chi_holds_chi(be):
     from lfm_b200 import Evolver, gravity_only
 
