@@ -179,12 +179,14 @@ int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* str
  * Process-wide; for tests and tuning. */
 int lfm_set_step_path(int path);
 
-/* Tile configuration of the fused kernel for (level, N): rows per tile,
- * shared-memory stages and planes per chunk (ic 0 = automatic).  tj <= 0
- * removes the entry and restores the built-in choice.  lfm_tune_get reports
- * the configuration the last step of that (level, N) ran with. */
-int lfm_tune_set(int level, int N, int tj, int stages, int ic);
-int lfm_tune_get(int level, int N, int* tj, int* stages, int* ic, int* threads, int* smem);
+/* Tile configuration of the fused kernel for (level, N): cells per thread
+ * along k (vec: 2 or 4, 0 = automatic), rows per tile, shared-memory stages
+ * and planes per chunk (ic 0 = automatic).  tj <= 0 removes the entry and
+ * restores the built-in choice.  lfm_tune_get reports the configuration the
+ * last fused step of that (level, N) ran with. */
+int lfm_tune_set(int level, int N, int vec, int tj, int stages, int ic);
+int lfm_tune_get(int level, int N, int* vec, int* tj, int* stages, int* ic, int* threads,
+                 int* smem);
 
 /* Reads (and optionally clears) the device status word that bounded
  * device-side waits set on timeout; synchronises the current device. */

@@ -119,6 +119,7 @@ lfm::MaskLut device_lut(const float* table, const lfm_mask_lut* lut) {
   m.shift = lut->shift;
   m.q_lo = lut->q_lo;
   m.q_hi = lut->q_hi;
+  m.count = lut->count;
   return m;
 }
 
@@ -126,6 +127,13 @@ int check_lut(const float* table, const lfm_mask_lut* lut, int N) {
   if (!lut) return fail(LFM_ERR_INVALID_ARG, "mask lookup table descriptor is null");
   if (lut->N != N) return fail(LFM_ERR_INVALID_ARG, "lookup table is for N=%d, step N=%d", lut->N, N);
   if (lut->count > 0 && !table) return fail(LFM_ERR_INVALID_ARG, "mask table pointer is null");
+  if (lut->shift != (N % 2 == 0 ? 3 : 2))
+    return fail(LFM_ERR_INVALID_ARG, "mask table shift %d does not match N=%d", lut->shift, N);
+  const int64_t want = lut->q_hi >= lut->q_lo
+                           ? (((int64_t)lut->q_hi - lut->q_lo) >> lut->shift) + 1 : 0;
+  if (lut->count != want)
+    return fail(LFM_ERR_INVALID_ARG, "mask table count %d, its key band holds %lld", lut->count,
+                (long long)want);
   return LFM_OK;
 }
 
@@ -248,9 +256,9 @@ int lfm_mask_lut_build(int N, const float* mask_host, float* table_host, int cap
   lfm_mask_lut d;
   d.N = N;
   d.shift = shift;
-  if (q_lo == INT32_MAX) {  // mask identically 0
+  if (q_lo == INT32_MAX) {  // mask identically 0: every key below the (empty) band
     d.q_lo = INT32_MAX;
-    d.q_hi = INT32_MAX;
+    d.q_hi = INT32_MAX - 1;
     d.count = 0;
   } else if (q_hi == INT32_MIN) {  // mask identically 1
     d.q_lo = 0;

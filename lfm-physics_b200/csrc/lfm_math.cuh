@@ -129,12 +129,22 @@ __device__ __forceinline__ float current_axis(float pr, float pi, float pr_p, fl
 struct MaskLut {
   const float* table;
   int32_t shift, q_lo, q_hi;
+  int32_t count;  // entries in `table`
 };
 
 __device__ __forceinline__ float mask_from_q(const MaskLut& m, int32_t q) {
   if (q < m.q_lo) return 0.0f;
   if (q > m.q_hi) return 1.0f;
   return __ldg(m.table + ((q - m.q_lo) >> m.shift));
+}
+
+// Branch-free variant: the table load is predicated on the band test, so a
+// warp does not diverge around it.
+__device__ __forceinline__ float mask_from_q_flat(const MaskLut& m, int32_t q) {
+  const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
+  float t = 0.0f;
+  if (in_band) t = __ldg(m.table + ((q - m.q_lo) >> m.shift));
+  return in_band ? t : (q < m.q_lo ? 0.0f : 1.0f);
 }
 
 // Squared doubled offset from the lattice centre: (2x - N + 1)^2.

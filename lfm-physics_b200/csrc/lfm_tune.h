@@ -10,6 +10,7 @@ struct TileConfig {
   int ic;       // planes per chunk (0 = automatic)
   int threads;  // CTA size (recorded)
   int smem;     // dynamic shared memory bytes (recorded)
+  int vec;      // cells per thread along k (0 = automatic)
 };
 
 bool tune_lookup(int level, int N, TileConfig* out);

@@ -91,6 +91,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+__device__ __forceinline__ uint32_t atom_add_acq_rel_cta(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.acq_rel.cta.shared::cta.add.u32 %0, [%1], %2;"
+               : "=r"(old)
+               : "r"(smem_addr(p)), "r"(v)
+               : "memory");
+  return old;
+}
+
+// Orders generic-proxy shared-memory accesses made before it (this thread's,
+// and the other warps' ones acquired through the counter) before the
+// async-proxy (TMA) writes issued after it.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 __device__ __forceinline__ uint64_t now_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -459,7 +475,298 @@ __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ T
   }
   if (abort_flag && tid == 0) {
     // Let the copies this CTA started finish before its shared memory goes away.
-    for (int u = waited; u < issued; ++u)
+    for (int u = max(waited, issued - S); u < issued; ++u)
+      mbar_wait_bounded(&bars[u % S], (uint32_t)((u / S) & 1), kDrainLimitNs);
+  }
+}
+
+// ---- register-queue kernel (REAL, COMPLEX) -------------------------------------
+//
+// Same tiles and copy ring as tma_step_kernel, but each plane of a stencil
+// field is read from shared memory once: the thread keeps, for the planes
+// i-1, i, i+1, the rows j-1, j, j+1 of its V cells in registers and rotates
+// them as it marches (the loop is unrolled by three so the rotation is a
+// renaming).  Neighbours k0-1 and k0+V are plain scalar loads.  A stage is
+// dead once its plane has been the centre plane, so it is refilled one plane
+// earlier than in tma_step_kernel: S stages keep S-2 planes in flight.
+template <int V>
+struct QPlane {
+  Vec<V> m, z, p;        // rows j-1, j, j+1
+  float zl, zr;          // row j at k0-1, k0+V
+  float ml, mr, pl, pr;  // rows j-1, j+1 at k0-1, k0+V (loaded when centre)
+};
+
+struct QLane {
+  int j, k0;                               // the thread's row and first cell
+  int o_m, o_z, o_p;                       // row offsets at k0 in a field block
+  int o_zl, o_zr, o_ml, o_mr, o_pl, o_pr;  // neighbour offsets
+  int o_pt;                                // point rows at k0 (from the stage base)
+};
+
+template <int V>
+__device__ __forceinline__ void q_load(QPlane<V>& q, const float* smem, int base, const QLane& L) {
+  q.m = lds<V>(smem, base + L.o_m);
+  q.z = lds<V>(smem, base + L.o_z);
+  q.p = lds<V>(smem, base + L.o_p);
+  q.zl = smem[base + L.o_zl];
+  q.zr = smem[base + L.o_zr];
+}
+
+template <int V>
+__device__ __forceinline__ void q_centre(QPlane<V>& q, const float* smem, int base,
+                                         const QLane& L) {
+  q.ml = smem[base + L.o_ml];
+  q.mr = smem[base + L.o_mr];
+  q.pl = smem[base + L.o_pl];
+  q.pr = smem[base + L.o_pr];
+}
+
+template <int V>
+__device__ __forceinline__ S19 q_s19(const QPlane<V>& M, const QPlane<V>& A, const QPlane<V>& P,
+                                     int e) {
+  S19 s;
+  s.c = A.z.v[e];
+  s.im = M.z.v[e];
+  s.ip = P.z.v[e];
+  s.jm = A.m.v[e];
+  s.jp = A.p.v[e];
+  s.km = e > 0 ? A.z.v[e - 1] : A.zl;
+  s.kp = e < V - 1 ? A.z.v[e + 1] : A.zr;
+  s.imjm = M.m.v[e];
+  s.imjp = M.p.v[e];
+  s.ipjm = P.m.v[e];
+  s.ipjp = P.p.v[e];
+  s.imkm = e > 0 ? M.z.v[e - 1] : M.zl;
+  s.imkp = e < V - 1 ? M.z.v[e + 1] : M.zr;
+  s.ipkm = e > 0 ? P.z.v[e - 1] : P.zl;
+  s.ipkp = e < V - 1 ? P.z.v[e + 1] : P.zr;
+  s.jmkm = e > 0 ? A.m.v[e - 1] : A.ml;
+  s.jmkp = e < V - 1 ? A.m.v[e + 1] : A.mr;
+  s.jpkm = e > 0 ? A.p.v[e - 1] : A.pl;
+  s.jpkp = e < V - 1 ? A.p.v[e + 1] : A.pr;
+  return s;
+}
+
+__device__ __forceinline__ Faces faces_of(const S19& s) {
+  Faces f;
+  f.im = s.im; f.ip = s.ip; f.jm = s.jm; f.jp = s.jp; f.km = s.km; f.kp = s.kp;
+  return f;
+}
+
+template <int LEVEL>
+struct QFields {
+  static constexpr int ns = (LEVEL == LFM_REAL) ? 2 : 3;
+};
+
+// Shared bookkeeping of the barrier-free march.
+struct QShared {
+  uint32_t done[kMaxStages];  // warps finished with the stage's current plane
+  int issued;                 // planes handed to the copy engine so far
+  int abort_flag;
+};
+
+// One plane of the march with the roles (prev, cur, next) = (PA, PB, PC) of
+// the register queue.  Warps do not wait for each other: each one releases
+// the centre plane's stage when it is done with it, and the last warp to do
+// so refills the stage with the plane S further on.  Returns false when the
+// CTA must stop (a bounded wait gave up).
+template <int LEVEL, int V, int PA, int PB, int PC>
+__device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_t* bars,
+                                        QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
+                                        const QLane& L, int c, int i0, int i1, int j0,
+                                        int nplanes, int nwarps, int& s_cur, int& s_nxt,
+                                        uint32_t& ph_nxt, int32_t qj, const int32_t (&qk)[V]) {
+  constexpr int NS = QFields<LEVEL>::ns;
+  const StepArgs& a = P.a;
+  const int N = P.N, TJ = P.TJ;
+  const int FB = (TJ + 2) * N;
+  const int PTS = TJ * N;  // point-field stride
+  const int SF = P.stage_floats;
+  if (*(volatile int*)&sh.abort_flag) return false;
+  if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
+    *(volatile int*)&sh.abort_flag = 1;
+    atomicOr(a.status, LFM_ERR_DEVICE_TIMEOUT);
+    return false;
+  }
+  const int bn = s_nxt * SF, bc = s_cur * SF;
+#pragma unroll
+  for (int f = 0; f < NS; ++f) {
+    q_load<V>(Q[f][PC], smem, bn + f * FB, L);
+    q_centre<V>(Q[f][PB], smem, bc + f * FB, L);
+  }
+  const int i = i0 + c;
+  const int j = L.j, k0 = L.k0;
+  float mask[V], absorb[V];
+  if (P.pf_mask >= 0) {
+    const Vec<V> m = lds<V>(smem, bc + L.o_pt + P.pf_mask * PTS);
+#pragma unroll
+    for (int e = 0; e < V; ++e) mask[e] = m.v[e];
+  } else {
+    const int32_t qij = qterm(i, N) + qj;
+#pragma unroll
+    for (int e = 0; e < V; ++e) mask[e] = mask_from_q_flat(a.lut, qij + qk[e]);
+  }
+#pragma unroll
+  for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
+  const int64_t gofs = ((int64_t)i * N + j) * N + k0;
+  if constexpr (LEVEL == LFM_REAL) {
+    const Vec<V> ep = lds<V>(smem, bc + L.o_pt);
+    const Vec<V> xp = lds<V>(smem, bc + L.o_pt + PTS);
+    float o_psi[V], o_chi[V], o_pp[V], o_cp[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const S19 E = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+      const S19 X = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+      const float epv = a.damp_prev ? fmul(ep.v[e], absorb[e]) : ep.v[e];
+      const RealOut o = real_cell(lap19(E), E.c, epv, lap19(X), X.c, xp.v[e], mask[e], a.c);
+      o_psi[e] = o.psi; o_chi[e] = o.chi; o_pp[e] = o.psi_prev; o_cp[e] = o.chi_prev;
+    }
+    stg<V>(a.pr_out + gofs, o_psi);
+    stg<V>(a.chi_out + gofs, o_chi);
+    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_pp);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
+  } else {
+    const Vec<V> rp = lds<V>(smem, bc + L.o_pt);
+    const Vec<V> ip = lds<V>(smem, bc + L.o_pt + PTS);
+    const Vec<V> xp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+    float o_r[V], o_i[V], o_c[V], o_rp[V], o_ip[V], o_cp[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const S19 R = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+      const S19 I = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+      const S19 X = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
+      const float rpv = a.damp_prev ? fmul(rp.v[e], absorb[e]) : rp.v[e];
+      const float ipv = a.damp_prev ? fmul(ip.v[e], absorb[e]) : ip.v[e];
+      const ComplexOut o = complex_cell(lap19(R), R.c, rpv, faces_of(R), lap19(I), I.c, ipv,
+                                        faces_of(I), lap19(X), X.c, xp.v[e], mask[e], a.c);
+      o_r[e] = o.pr; o_i[e] = o.pi; o_c[e] = o.chi;
+      o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev; o_cp[e] = o.chi_prev;
+    }
+    stg<V>(a.pr_out + gofs, o_r);
+    stg<V>(a.pi_out + gofs, o_i);
+    stg<V>(a.chi_out + gofs, o_c);
+    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_rp);
+    if (a.pi_prev_out) stg<V>(a.pi_prev_out + gofs, o_ip);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
+  }
+  // Release the centre plane's stage (u = c+1); the last warp refills it
+  // with u = c+1+S.
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    const uint32_t before = atom_add_acq_rel_cta(&sh.done[s_cur], 1u);
+    if (before == (uint32_t)(nwarps - 1)) {
+      sh.done[s_cur] = 0u;
+      fence_proxy_async_smem();
+      if (c + 1 + P.S < nplanes) {
+        issue_plane(P, smem, bars, c + 1 + P.S, i0, i1, j0);
+        atomicMax(&sh.issued, c + 2 + P.S);
+      }
+    }
+  }
+  __syncwarp();
+  s_cur = s_nxt;
+  s_nxt = (s_nxt + 1 == P.S) ? 0 : s_nxt + 1;
+  if (s_nxt == 0) ph_nxt ^= 1u;
+  return true;
+}
+
+template <int LEVEL, int V>
+__global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
+  constexpr int NS = QFields<LEVEL>::ns;
+  extern __shared__ __align__(128) float smem[];
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  __shared__ QShared sh;
+
+  const int N = P.N, TJ = P.TJ, S = P.S;
+  const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
+  const int j0 = jt * TJ;
+  const int i0 = ch * P.IC;
+  const int i1 = min(i0 + P.IC, N);
+  const int n = i1 - i0;
+  const int nplanes = n + 2;
+  const int tid = threadIdx.x;
+  const int nwarps = blockDim.x >> 5;
+  const int tpr = N / V;
+  const int r = tid / tpr;
+  const int k0 = (tid % tpr) * V;
+  const int km1 = (k0 == 0) ? N - 1 : k0 - 1;
+  const int kpv = (k0 + V == N) ? 0 : k0 + V;
+  QLane L;
+  L.j = j0 + r;
+  L.k0 = k0;
+  L.o_m = r * N + k0;
+  L.o_z = (r + 1) * N + k0;
+  L.o_p = (r + 2) * N + k0;
+  L.o_zl = (r + 1) * N + km1;
+  L.o_zr = (r + 1) * N + kpv;
+  L.o_ml = r * N + km1;
+  L.o_mr = r * N + kpv;
+  L.o_pl = (r + 2) * N + km1;
+  L.o_pr = (r + 2) * N + kpv;
+  L.o_pt = NS * (TJ + 2) * N + r * N + k0;
+  const int32_t qj = qterm(j0 + r, N);
+  int32_t qk[V];
+#pragma unroll
+  for (int e = 0; e < V; ++e) qk[e] = qterm(k0 + e, N);
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&bars[s], 1);
+      sh.done[s] = 0u;
+    }
+    sh.abort_flag = 0;
+    sh.issued = 0;
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int first = min(S, nplanes);
+    for (int u = 0; u < first; ++u) issue_plane(P, smem, bars, u, i0, i1, j0);
+    sh.issued = first;
+  }
+  QPlane<V> Q[NS][3];
+  // planes i0-1 (u = 0, stage 0) and i0 (u = 1, stage 1): both first uses, parity 0
+  bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitLimitNs);
+  ok = mbar_wait_bounded(&bars[1 % S], 0u, kWaitLimitNs) && ok;
+  if (!ok) {
+    sh.abort_flag = 1;
+    atomicOr(P.a.status, LFM_ERR_DEVICE_TIMEOUT);
+  } else {
+#pragma unroll
+    for (int f = 0; f < NS; ++f) {
+      q_load<V>(Q[f][0], smem, 0 * P.stage_floats + f * (TJ + 2) * N, L);
+      q_load<V>(Q[f][1], smem, (1 % S) * P.stage_floats + f * (TJ + 2) * N, L);
+    }
+  }
+  __syncthreads();
+  if (!sh.abort_flag) {
+    // stage 0 (plane i0-1) is dead: refill it with u = S
+    if (tid == 0 && S < nplanes) {
+      fence_proxy_async_smem();
+      issue_plane(P, smem, bars, S, i0, i1, j0);
+      sh.issued = S + 1;
+    }
+    int s_cur = 1 % S, s_nxt = 2 % S;
+    uint32_t ph_nxt = (uint32_t)((2 / S) & 1);
+    int c = 0;
+    while (true) {
+      if (c >= n || !q_plane<LEVEL, V, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes,
+                                                nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+        break;
+      if (++c >= n || !q_plane<LEVEL, V, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+                                                  nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+        break;
+      if (++c >= n || !q_plane<LEVEL, V, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+                                                  nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+        break;
+      ++c;
+    }
+  }
+  if (*(volatile int*)&sh.abort_flag && (tid & 31) == 0) {
+    // The last use of each stage is the only one that can still be in flight;
+    // let it land before this CTA's shared memory goes away.
+    const int issued = *(volatile int*)&sh.issued;
+    for (int u = max(0, issued - S); u < issued; ++u)
       mbar_wait_bounded(&bars[u % S], (uint32_t)((u / S) & 1), kDrainLimitNs);
   }
 }
@@ -475,27 +782,44 @@ constexpr int kSmemLimit = 226 * 1024;
 
 int stage_bytes(int N, int TJ, int ns, int np) { return 4 * N * (ns * (TJ + 2) + np * TJ); }
 
-Choice choose(int level, int N, int V, int ns, int np) {
+// Shared-memory carveouts an SM can be configured with (KB); the rest of the
+// 256 KB L1/shared array is L1 cache, which holds the sponge lookup table.
+int carveout_kb(int bytes) {
+  static const int kCarve[] = {0, 8, 16, 32, 64, 100, 132, 164, 196, 228};
+  for (int c : kCarve)
+    if (bytes <= c * 1024) return c;
+  return 228;
+}
+
+// extra_smem: bytes of shared memory beyond the stage ring (the mask table
+// when it is staged there); l1_table_bytes: a table read through L1 that the
+// carveout must leave room for (0 when none).
+Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threads,
+              int regs, const TileConfig* forced, int extra_smem, int l1_table_bytes) {
   Choice best;
   double best_score = -1.0;
   const int tpr = N / V;
-  TileConfig forced;
-  const bool have_forced = tune_lookup(level, N, &forced);
+  const int min_s = queue ? 3 : 4;  // stages live at once: 2 (queue) or 3
   for (int TJ = 1; TJ <= N; ++TJ) {
     if (N % TJ) continue;
     const int threads = TJ * tpr;
-    if (threads % 32 || threads < 64 || threads > 512) continue;
-    for (int S = 4; S <= kMaxStages; ++S) {
-      const int smem = S * stage_bytes(N, TJ, ns, np);
+    if (threads % 32 || threads < 64 || threads > max_threads) continue;
+    for (int S = min_s; S <= kMaxStages; ++S) {
+      const int smem = S * stage_bytes(N, TJ, ns, np) + extra_smem;
       if (smem > kSmemLimit) continue;
-      if (have_forced && (forced.tj != TJ || forced.stages != S)) continue;
+      if (forced && (forced->tj != TJ || forced->stages != S)) continue;
       const int cta_by_smem = (228 * 1024) / (smem + 1024);
       const int cta_by_thr = 2048 / threads;
-      const int ctas = std::max(1, std::min(cta_by_smem, cta_by_thr));
+      const int cta_by_reg = 65536 / std::max(1, regs * threads);
+      const int ctas = std::max(1, std::min(std::min(cta_by_smem, cta_by_thr), cta_by_reg));
       const double warps = std::min(ctas * threads / 32, 48);
-      const double halo = (double)TJ / (TJ + 2);            // useful fraction of stencil rows
-      const double depth = std::min(S - 3, 2) / 2.0;        // planes streamed ahead
-      const double score = warps / 48.0 + 0.6 * halo + 0.25 * depth;
+      const double halo = (double)TJ / (TJ + 2);  // useful fraction of stencil rows
+      const double depth = std::min(S - (min_s - 1), 2) / 2.0;  // planes streamed ahead
+      // L1 left beside the shared-memory carveout must hold the mask table
+      const int l1_kb = 256 - carveout_kb(ctas * (smem + 1024));
+      // (measured at 512^3: a 60-92 KB L1 beside the 67 KB table runs 10-15% slower)
+      const bool table_fits = l1_table_bytes == 0 || l1_kb * 1024 >= l1_table_bytes + 48 * 1024;
+      const double score = warps / 48.0 + 0.6 * halo + 0.25 * depth + (table_fits ? 0.5 : 0.0);
       if (score > best_score) {
         best_score = score;
         best.TJ = TJ;
@@ -507,9 +831,11 @@ Choice choose(int level, int N, int V, int ns, int np) {
   }
   if (!best.TJ) return best;
   const int JT = N / best.TJ;
-  const int ctas = std::max(1, std::min((228 * 1024) / (best.smem + 1024), 2048 / best.threads));
-  if (have_forced && forced.ic > 0) {
-    best.IC = std::min(forced.ic, N);
+  const int ctas = std::max(1, std::min(std::min((228 * 1024) / (best.smem + 1024),
+                                                 2048 / best.threads),
+                                        65536 / std::max(1, regs * best.threads)));
+  if (forced && forced->ic > 0) {
+    best.IC = std::min(forced->ic, N);
   } else {
     // Planes per chunk: balance the last wave of tiles over 148 SMs against
     // the two halo planes each chunk loads in addition to its own.
@@ -529,33 +855,81 @@ Choice choose(int level, int N, int V, int ns, int np) {
   return best;
 }
 
-template <int LEVEL, int V>
-cudaError_t launch_level(const TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  // Raise the kernel's dynamic shared-memory limit to what this launch needs,
-  // within the device's opt-in limit less the kernel's static shared memory.
-  static std::mutex mu;
-  static int granted = 0;
+template <typename K>
+cudaError_t kernel_regs(K kernel, int* regs) {
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  *regs = fa.numRegs;
+  return e;
+}
+
+// Raises the kernel's dynamic shared-memory limit to what the launch needs
+// (within the device's opt-in limit less its static shared memory) and launches.
+template <typename K>
+cudaError_t launch_kernel(K kernel, int* granted, std::mutex* mu, const TmaParams& P,
+                          const Choice& ch, cudaStream_t stream) {
   {
-    std::lock_guard<std::mutex> lk(mu);
-    if (ch.smem > granted) {
+    std::lock_guard<std::mutex> lk(*mu);
+    if (ch.smem > *granted) {
       int dev = 0, optin = 0;
       cudaError_t e = cudaGetDevice(&dev);
       if (e == cudaSuccess)
         e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
       cudaFuncAttributes fa{};
-      if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, tma_step_kernel<LEVEL, V>);
+      if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
       if (e != cudaSuccess) return e;
       if (ch.smem + (int)fa.sharedSizeBytes > optin) return cudaErrorNotSupported;
-      e = cudaFuncSetAttribute(tma_step_kernel<LEVEL, V>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, ch.smem);
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, ch.smem);
       if (e != cudaSuccess) return e;
-      granted = ch.smem;
+      *granted = ch.smem;
     }
   }
   const int JT = P.N / P.TJ;
   const int chunks = (P.N + P.IC - 1) / P.IC;
-  tma_step_kernel<LEVEL, V><<<JT * chunks, ch.threads, ch.smem, stream>>>(P);
+  kernel<<<JT * chunks, ch.threads, ch.smem, stream>>>(P);
   return cudaGetLastError();
+}
+
+template <int LEVEL, int V, bool QUEUE>
+struct KernelSlot {
+  static std::mutex mu;
+  static int granted;
+  static auto fn() {
+    if constexpr (QUEUE)
+      return tma_queue_kernel<LEVEL, V>;
+    else
+      return tma_step_kernel<LEVEL, V>;
+  }
+};
+template <int LEVEL, int V, bool QUEUE>
+std::mutex KernelSlot<LEVEL, V, QUEUE>::mu;
+template <int LEVEL, int V, bool QUEUE>
+int KernelSlot<LEVEL, V, QUEUE>::granted = 0;
+
+template <int LEVEL, int V, bool QUEUE>
+cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t stream) {
+  using Slot = KernelSlot<LEVEL, V, QUEUE>;
+  int regs = 0;
+  cudaError_t e = kernel_regs(Slot::fn(), &regs);
+  if (e != cudaSuccess) return e;
+  // threads per CTA the register file can hold (at least one CTA per SM)
+  const int max_threads = std::min(512, (65536 / std::max(regs, 1)) / 32 * 32);
+  // The mask table is read through L1: keep the shared-memory carveout small
+  // enough to leave L1 room for it (measured: staging it in shared memory
+  // instead is slower, bank conflicts of the random-key loads).
+  const int count = (P.pf_mask >= 0) ? 0 : P.a.lut.count;
+  const int table_bytes = 4 * count;
+  const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0,
+                           table_bytes);
+  if (!ch.TJ) return cudaErrorNotSupported;
+  P.TJ = ch.TJ;
+  P.S = ch.S;
+  P.IC = ch.IC;
+  P.JT = P.N / ch.TJ;
+  P.stage_floats = stage_bytes(P.N, ch.TJ, P.ns, P.np) / 4;
+  TileConfig used{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem, V};
+  tune_record(LEVEL, P.N, used);
+  return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -565,7 +939,6 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   const int N = a.N;
   if (N % 4 != 0 || N < 8) return cudaErrorNotSupported;
-  const int V = (a.level == LFM_COLOR) ? 2 : 4;
   TmaParams P{};
   P.a = a;
   P.N = N;
@@ -609,19 +982,22 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   for (const void* p : ptrs)
     if (p && !aligned16(p)) return cudaErrorNotSupported;
 
-  const Choice ch = choose(a.level, N, V, P.ns, P.np);
-  if (!ch.TJ) return cudaErrorNotSupported;
-  P.TJ = ch.TJ;
-  P.S = ch.S;
-  P.IC = ch.IC;
-  P.JT = N / ch.TJ;
-  P.stage_floats = ch.smem / (4 * ch.S);
-  tune_record(a.level, N, TileConfig{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem});
-  switch (a.level) {
-    case LFM_REAL: return launch_level<LFM_REAL, 4>(P, ch, stream);
-    case LFM_COMPLEX: return launch_level<LFM_COMPLEX, 4>(P, ch, stream);
-    default: return launch_level<LFM_COLOR, 2>(P, ch, stream);
+  TileConfig forced_cfg;
+  const bool have_forced = tune_lookup(a.level, N, &forced_cfg);
+  const TileConfig* forced = have_forced ? &forced_cfg : nullptr;
+  if (a.level == LFM_REAL) {
+    const int v = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 4;
+    if (N % v) return cudaErrorNotSupported;
+    return v == 2 ? plan_and_launch<LFM_REAL, 2, true>(P, forced, stream)
+                  : plan_and_launch<LFM_REAL, 4, true>(P, forced, stream);
   }
+  if (a.level == LFM_COMPLEX) {
+    const int v = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 2;
+    if (N % v) return cudaErrorNotSupported;
+    return v == 4 ? plan_and_launch<LFM_COMPLEX, 4, true>(P, forced, stream)
+                  : plan_and_launch<LFM_COMPLEX, 2, true>(P, forced, stream);
+  }
+  return plan_and_launch<LFM_COLOR, 2, false>(P, forced, stream);
 }
 
 }  // namespace lfm

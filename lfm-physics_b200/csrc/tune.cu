@@ -30,21 +30,24 @@ void tune_record(int level, int N, const TileConfig& used) {
 
 extern "C" {
 
-int lfm_tune_set(int level, int N, int tj, int stages, int ic) {
+int lfm_tune_set(int level, int N, int vec, int tj, int stages, int ic) {
   if (level < 0 || level > 2 || N < 2) return LFM_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(lfm::g_mu);
   if (tj <= 0) {
     lfm::g_forced.erase({level, N});
     return LFM_OK;
   }
-  lfm::g_forced[{level, N}] = lfm::TileConfig{tj, stages, ic, 0, 0};
+  if (vec != 0 && vec != 2 && vec != 4) return LFM_ERR_INVALID_ARG;
+  lfm::g_forced[{level, N}] = lfm::TileConfig{tj, stages, ic, 0, 0, vec};
   return LFM_OK;
 }
 
-int lfm_tune_get(int level, int N, int* tj, int* stages, int* ic, int* threads, int* smem) {
+int lfm_tune_get(int level, int N, int* vec, int* tj, int* stages, int* ic, int* threads,
+                 int* smem) {
   std::lock_guard<std::mutex> lk(lfm::g_mu);
   auto it = lfm::g_used.find({level, N});
   if (it == lfm::g_used.end()) return LFM_ERR_INVALID_ARG;
+  if (vec) *vec = it->second.vec;
   if (tj) *tj = it->second.tj;
   if (stages) *stages = it->second.stages;
   if (ic) *ic = it->second.ic;

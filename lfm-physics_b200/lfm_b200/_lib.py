@@ -58,8 +58,8 @@ _SIGNATURES = {
     "lfm_helmholtz_sa_f32": [_P] * 4 + [c_int, _D, _D, _P],
     "lfm_sa_clip_f32": [_P, _P, c_int64, _P],
     "lfm_device_status": [POINTER(c_int), c_int],
-    "lfm_tune_set": [c_int] * 5,
-    "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 5,
+    "lfm_tune_set": [c_int] * 6,
+    "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 6,
 }
 
 _lib = None
@@ -108,18 +108,18 @@ def set_step_path(path: int) -> None:
     call("lfm_set_step_path", int(path))
 
 
-def tune_set(level: int, N: int, tj: int, stages: int, ic: int = 0) -> None:
+def tune_set(level: int, N: int, tj: int, stages: int, ic: int = 0, vec: int = 0) -> None:
     """Force the fused kernel's tile configuration for (level, N); tj <= 0 clears it."""
-    call("lfm_tune_set", int(level), int(N), int(tj), int(stages), int(ic))
+    call("lfm_tune_set", int(level), int(N), int(vec), int(tj), int(stages), int(ic))
 
 
 def tune_get(level: int, N: int) -> dict | None:
     """The tile configuration the last fused step of (level, N) used, or None."""
-    vals = [c_int(0) for _ in range(5)]
+    vals = [c_int(0) for _ in range(6)]
     rc = load().lfm_tune_get(int(level), int(N), *[ctypes.byref(v) for v in vals])
     if rc != LFM_OK:
         return None
-    return dict(zip(("tj", "stages", "ic", "threads", "smem"), (v.value for v in vals)))
+    return dict(zip(("vec", "tj", "stages", "ic", "threads", "smem"), (v.value for v in vals)))
 
 
 def device_status(clear: bool = True) -> int:

@@ -80,7 +80,7 @@ class MaskTable:
         d = _lib.MaskLut()
         d.N, d.shift = N, shift
         if nz.size == 0:
-            d.q_lo, d.q_hi, d.count = np.iinfo(np.int32).max, np.iinfo(np.int32).max, 0
+            d.q_lo, d.q_hi, d.count = np.iinfo(np.int32).max, np.iinfo(np.int32).max - 1, 0
             table = np.zeros(1, np.float32)
         elif n1.size == 0:
             d.q_lo, d.q_hi, d.count = 0, -1, 0

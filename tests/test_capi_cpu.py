@@ -109,6 +109,7 @@ def test_mask_table_edge_cases(lib):
     N = 10
     zero = MaskTable.from_mask(N, np.zeros(N**3, np.float32))
     assert (zero.lookup(radial_keys(N)) == 0).all()
+    assert zero.desc.count == 0 and zero.desc.q_hi < zero.desc.q_lo
     one = MaskTable.from_mask(N, np.ones(N**3, np.float32))
     assert (one.lookup(radial_keys(N)) == 1).all()
 
