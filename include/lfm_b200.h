@@ -173,6 +173,25 @@ int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_
                          float* sa_raw, int N, double sa_gamma, double sa_d, void* stream);
 int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Float64 metrics of a state, reduced on the device (replaces the host
+ * compute_metrics of lfm/analysis/metrics.py:29-111 except the cluster
+ * count; energy terms as lfm/analysis/energy.py:26-113 with np.gradient's
+ * non-periodic edges; chi statistics over interior_mask,
+ * lfm/analysis/structure.py:148-171).  psi_*_prev may be NULL (kinetic 0);
+ * psi_i* are NULL at the REAL level; colour arrays hold 3 components.
+ * out_host[LFM_METRICS_COUNT] receives, in order: energy_kinetic,
+ * energy_gradient, energy_potential, energy_total, chi_min, chi_max,
+ * chi_mean, chi_std, well_fraction, void_fraction, psi_sq_total,
+ * interior_cells, nonfinite_cells.  Synchronises `stream`.  Scratch for the
+ * per-CTA partials lives in `ctx`.
+ * ------------------------------------------------------------------------ */
+#define LFM_METRICS_COUNT 13
+int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float* psi_r_prev,
+                    const float* psi_i, const float* psi_i_prev, const float* chi, int N,
+                    double dt, double c, double boundary_fraction, double well_threshold,
+                    double void_threshold, double* out_host, void* stream);
+
 /* Kernel path for the step calls: 0 = automatic (fused 2.5D kernel where
  * it applies, the direct kernel otherwise), 1 = direct kernel only,
  * 2 = fused kernel only (calls it cannot serve return LFM_ERR_UNSUPPORTED).

@@ -16,6 +16,7 @@
 
 #include "lfm_b200.h"
 #include "lfm_kernels.h"
+#include "lfm_metrics.h"
 
 // Device status word: bounded device-side waits OR an LFM_ERR_* code into
 // it when they give up (read back with lfm_device_status).
@@ -152,6 +153,7 @@ struct lfm_context {
   int device = 0;
   std::mutex mu;
   std::map<int, FftSlot> slots;
+  double* metric_partials = nullptr;  // kMetricRows x kPartialStride, then the final row
 };
 
 namespace {
@@ -429,6 +431,7 @@ int lfm_context_destroy(lfm_context* ctx) {
     if (kv.second.spec) cudaFree(kv.second.spec);
     if (kv.second.sa_raw) cudaFree(kv.second.sa_raw);
   }
+  if (ctx->metric_partials) cudaFree(ctx->metric_partials);
   cudaSetDevice(prev);
   delete ctx;
   return LFM_OK;
@@ -532,6 +535,107 @@ int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* str
   if (count == 0) return LFM_OK;
   cudaError_t e = lfm::launch_clip(sa_raw, sa_out, count, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "clip launch");
+  return LFM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Turns the reduced sums into the metrics of lfm_metrics_f64.
+void finish_metrics(const double* r, double chi_shift, double* out) {
+  const double count = r[lfm::kCount];
+  out[0] = r[lfm::kKinetic];
+  out[1] = r[lfm::kGradient];
+  out[2] = r[lfm::kPotential];
+  out[3] = out[0] + out[1] + out[2];
+  if (count > 0) {
+    const double mean_d = r[lfm::kChiSum] / count;
+    double var = r[lfm::kChiSq] / count - mean_d * mean_d;
+    if (var < 0) var = 0;
+    out[4] = r[lfm::kMetricSums];
+    out[5] = r[lfm::kMetricSums + 1];
+    out[6] = chi_shift + mean_d;
+    out[7] = sqrt(var);
+    out[8] = r[lfm::kWell] / count;
+    out[9] = r[lfm::kVoid] / count;
+  } else {
+    for (int q = 4; q < 10; ++q) out[q] = 0.0;
+  }
+  out[10] = r[lfm::kPsiSq];
+  out[11] = count;
+  out[12] = r[lfm::kNonFinite];
+}
+
+int check_metrics_args(int level, const float* psi_r, const float* psi_i, const float* chi, int N,
+                       double dt, double boundary_fraction, double* out_host) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (level < 0 || level > 2) return fail(LFM_ERR_INVALID_ARG, "level %d", level);
+  if (!psi_r || !chi || !out_host || (level > 0 && !psi_i))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  if (!(dt > 0)) return fail(LFM_ERR_INVALID_ARG, "dt must be positive");
+  if (!(boundary_fraction >= 0 && boundary_fraction <= 1))
+    return fail(LFM_ERR_INVALID_ARG, "boundary_fraction %g outside [0, 1]", boundary_fraction);
+  return LFM_OK;
+}
+
+lfm::MetricsArgs metrics_args(int level, const float* psi_r, const float* psi_r_prev,
+                              const float* psi_i, const float* psi_i_prev, const float* chi,
+                              int N, double dt, double c, double boundary_fraction,
+                              double well_threshold, double void_threshold) {
+  lfm::MetricsArgs a{};
+  a.level = level;
+  a.N = N;
+  a.pr = psi_r;
+  a.pr_prev = psi_r_prev;
+  a.pi = level > 0 ? psi_i : nullptr;
+  a.pi_prev = level > 0 ? psi_i_prev : nullptr;
+  a.chi = chi;
+  a.dt = dt;
+  a.c2 = c * c;
+  a.radius = (N / 2.0) * (1.0 - boundary_fraction);
+  a.chi_shift = 19.0;
+  a.well = (float)well_threshold;
+  a.void_thr = (float)void_threshold;
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float* psi_r_prev,
+                    const float* psi_i, const float* psi_i_prev, const float* chi, int N,
+                    double dt, double c, double boundary_fraction, double well_threshold,
+                    double void_threshold, double* out_host, void* stream) {
+  if (!ctx) return fail(LFM_ERR_INVALID_ARG, "null context");
+  int rc = check_metrics_args(level, psi_r, psi_i, chi, N, dt, boundary_fraction, out_host);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != ctx->device)
+    return fail(LFM_ERR_INVALID_ARG, "context belongs to device %d, current device is %d",
+                ctx->device, dev);
+  if (!ctx->metric_partials) {
+    e = cudaMalloc(&ctx->metric_partials,
+                   sizeof(double) * (lfm::kMetricRows + 1) * lfm::kPartialStride);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc metric partials");
+  }
+  const lfm::MetricsArgs a = metrics_args(level, psi_r, psi_r_prev, psi_i, psi_i_prev, chi, N,
+                                          dt, c, boundary_fraction, well_threshold,
+                                          void_threshold);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* final_row = ctx->metric_partials + (size_t)lfm::kMetricRows * lfm::kPartialStride;
+  e = lfm::launch_metrics(a, ctx->metric_partials, lfm::kMetricRows, final_row, st);
+  if (e != cudaSuccess) return cuda_fail(e, "metrics launch");
+  double r[lfm::kPartialStride];
+  e = cudaMemcpyAsync(r, final_row, sizeof r, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "metrics readback");
+  finish_metrics(r, a.chi_shift, out_host);
   return LFM_OK;
 }
 

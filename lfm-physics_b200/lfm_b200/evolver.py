@@ -336,6 +336,32 @@ class Evolver:
             out["psi_i_prev"] = self._shape(self._prev_psi_view(True))
         return out
 
+    def metrics(self, prev=None, clusters: bool = False) -> dict:
+        """Float64 metrics of the current state, reduced on the device.
+
+        prev: None uses the leapfrog previous field for the kinetic term
+        (dPsi/dt over one step); pass device tensors to use another snapshot.
+        clusters: also count |Psi|^2 clusters on the host (one N^3 copy).
+        """
+        from .metrics import device_metrics, interior_mask, n_clusters
+
+        st = self.device_state()
+        if prev is None:
+            pr_prev, pi_prev = st["psi_r_prev"], st.get("psi_i_prev")
+        else:
+            pr_prev, pi_prev = prev
+        cfg = self.config
+        m = device_metrics(self.backend.context.handle, int(self._level), self.N,
+                           st["psi_r"].contiguous(), pr_prev.contiguous(),
+                           st["psi_i"].contiguous() if self._has_imag else None,
+                           pi_prev.contiguous() if pi_prev is not None else None,
+                           st["chi"].contiguous(), cfg.dt, getattr(cfg, "c", 1.0),
+                           cfg.boundary_fraction)
+        if clusters:
+            e = self.get_energy_density().astype(np.float64)
+            m["n_clusters"] = float(n_clusters(e, interior_mask(self.N, cfg.boundary_fraction)))
+        return m
+
     # ------------------------------------------------------------------
     # host accessors (evolver.py:289-536)
     # ------------------------------------------------------------------
