@@ -192,6 +192,24 @@ int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float
                     double dt, double c, double boundary_fraction, double well_threshold,
                     double void_threshold, double* out_host, void* stream);
 
+/* The metrics of lfm_metrics_f64 without any device allocation.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc --
+ * a process whose device memory is held by another allocator (a caching
+ * allocator such as PyTorch's can keep the free memory to itself), or a
+ * program that must not allocate after start-up -- and that therefore hold
+ * no lfm_context.  The per-CTA partials go to a static device array of about
+ * 240 KB that every GPU loading the library keeps until the process ends;
+ * lattices up to 512^3 cells fit, larger ones return LFM_ERR_CAPACITY.  The
+ * first call on each device looks up the array's device address and should
+ * come before any stream capture on that device.  All calls share the array:
+ * calls that overlap on the GPU (two streams, two threads) race; serialise
+ * them.  Same outputs, in the same order, as lfm_metrics_f64. */
+int lfm_metrics_f64_noalloc(int level, const float* psi_r, const float* psi_r_prev,
+                            const float* psi_i, const float* psi_i_prev, const float* chi, int N,
+                            double dt, double c, double boundary_fraction,
+                            double well_threshold, double void_threshold, double* out_host,
+                            void* stream);
+
 /* Kernel path for the step calls: 0 = automatic (fused 2.5D kernel where
  * it applies, the direct kernel otherwise), 1 = direct kernel only,
  * 2 = fused kernel only (calls it cannot serve return LFM_ERR_UNSUPPORTED).

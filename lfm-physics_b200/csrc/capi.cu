@@ -603,6 +603,31 @@ lfm::MetricsArgs metrics_args(int level, const float* psi_r, const float* psi_r_
 
 }  // namespace
 
+namespace lfm {
+
+// Argument checks, kernel arguments and host finishing of the metrics, for
+// entry points defined in other files (lfm_metrics_f64_noalloc).
+int metrics_prepare(int level, const float* psi_r, const float* psi_r_prev, const float* psi_i,
+                    const float* psi_i_prev, const float* chi, int N, double dt, double c,
+                    double boundary_fraction, double well_threshold, double void_threshold,
+                    double* out_host, MetricsArgs* out) {
+  const int rc = check_metrics_args(level, psi_r, psi_i, chi, N, dt, boundary_fraction, out_host);
+  if (rc) return rc;
+  *out = metrics_args(level, psi_r, psi_r_prev, psi_i, psi_i_prev, chi, N, dt, c,
+                      boundary_fraction, well_threshold, void_threshold);
+  return LFM_OK;
+}
+
+void metrics_finish(const double* sums, double chi_shift, double* out_host) {
+  finish_metrics(sums, chi_shift, out_host);
+}
+
+int abi_fail(int code, const char* detail) { return fail(code, "%s", detail); }
+
+int abi_cuda_fail(cudaError_t e, const char* what) { return cuda_fail(e, what); }
+
+}  // namespace lfm
+
 extern "C" {
 
 int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float* psi_r_prev,

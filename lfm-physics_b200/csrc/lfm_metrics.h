@@ -42,4 +42,14 @@ struct MetricsArgs {
 cudaError_t launch_metrics(const MetricsArgs& a, double* partials, int rows, double* out,
                            cudaStream_t stream);
 
+// Defined in capi.cu: the shared argument checks and host finishing of the
+// metrics entry points, and the thread's error detail.
+int metrics_prepare(int level, const float* psi_r, const float* psi_r_prev, const float* psi_i,
+                    const float* psi_i_prev, const float* chi, int N, double dt, double c,
+                    double boundary_fraction, double well_threshold, double void_threshold,
+                    double* out_host, MetricsArgs* out);
+void metrics_finish(const double* sums, double chi_shift, double* out_host);
+int abi_fail(int code, const char* detail);
+int abi_cuda_fail(cudaError_t e, const char* what);
+
 }  // namespace lfm

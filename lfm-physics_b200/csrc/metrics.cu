@@ -13,6 +13,10 @@
 // Each CTA reduces its cells to one row of partials in the scratch buffer; a
 // second single-CTA kernel reduces the rows in a fixed order, so results are
 // deterministic for a given grid.
+#include <cstdio>
+#include <mutex>
+
+#include "lfm_b200.h"
 #include "lfm_kernels.h"
 #include "lfm_metrics.h"
 
@@ -189,3 +193,87 @@ cudaError_t launch_metrics(const MetricsArgs& a, double* partials, int rows, dou
 }
 
 }  // namespace lfm
+
+// ---------------------------------------------------------------------------
+// Metrics without allocation (lfm_metrics_f64_noalloc).
+//
+// For callers that cannot allocate device memory: a process whose device
+// memory is all held by another allocator (PyTorch's caching allocator can
+// leave cudaMalloc failing while it keeps free blocks for itself), or a host
+// program that allocates only at start-up and must not call cudaMalloc
+// afterwards.  Such callers also hold no lfm_context, which is where
+// lfm_metrics_f64 keeps its scratch.
+//
+// The per-CTA partials live in this file-scope device array instead.  Every
+// GPU that loads the library holds it (about 240 KB) until the process ends.
+// One CTA reduces each 65536 cells, so a lattice may have at most
+// kNoAllocRows * 65536 cells (N <= 512).  Host code must not pass the
+// array's name to a kernel: on the host it only stands in for the symbol, and
+// the device address comes from cudaGetSymbolAddress, taken once per device
+// on the first call made with that device current.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocRows = 2048;
+constexpr long long kNoAllocCellsPerRow = 65536;
+
+static __device__ __align__(256) double g_noalloc_partials[(kNoAllocRows + 1) *
+                                                           lfm::kPartialStride];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return lfm::abi_cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return lfm::abi_fail(LFM_ERR_UNSUPPORTED, "device index outside the scratch table");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    double* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_partials);
+    if (e != cudaSuccess) return lfm::abi_cuda_fail(e, "cudaGetSymbolAddress(metric scratch)");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return LFM_OK;
+}
+
+}  // namespace
+
+extern "C" int lfm_metrics_f64_noalloc(int level, const float* psi_r, const float* psi_r_prev,
+                                       const float* psi_i, const float* psi_i_prev,
+                                       const float* chi, int N, double dt, double c,
+                                       double boundary_fraction, double well_threshold,
+                                       double void_threshold, double* out_host, void* stream) {
+  lfm::MetricsArgs a{};
+  int rc = lfm::metrics_prepare(level, psi_r, psi_r_prev, psi_i, psi_i_prev, chi, N, dt, c,
+                                boundary_fraction, well_threshold, void_threshold, out_host, &a);
+  if (rc) return rc;
+  const long long cells = (long long)N * N * N;
+  const long long rows = (cells + kNoAllocCellsPerRow - 1) / kNoAllocCellsPerRow;
+  if (rows > kNoAllocRows) {
+    char msg[160];
+    snprintf(msg, sizeof msg,
+             "N=%d needs %lld partial rows; the static scratch holds %d (lattices up to 512^3)",
+             N, rows, kNoAllocRows);
+    return lfm::abi_fail(LFM_ERR_CAPACITY, msg);
+  }
+  double* scratch = nullptr;
+  rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  // Every partial row and the final row are written before they are read,
+  // so nothing left in the array by an earlier call needs clearing.
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* final_row = scratch + (size_t)kNoAllocRows * lfm::kPartialStride;
+  cudaError_t e = lfm::launch_metrics(a, scratch, (int)rows, final_row, st);
+  if (e != cudaSuccess) return lfm::abi_cuda_fail(e, "metrics launch");
+  double r[lfm::kPartialStride];
+  e = cudaMemcpyAsync(r, final_row, sizeof r, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return lfm::abi_cuda_fail(e, "metrics readback");
+  lfm::metrics_finish(r, a.chi_shift, out_host);
+  return LFM_OK;
+}

@@ -59,6 +59,7 @@ _SIGNATURES = {
     "lfm_sa_clip_f32": [_P, _P, c_int64, _P],
     "lfm_device_status": [POINTER(c_int), c_int],
     "lfm_metrics_f64": [_P, c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
+    "lfm_metrics_f64_noalloc": [c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
     "lfm_tune_set": [c_int] * 6,
     "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 6,
 }
