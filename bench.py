@@ -51,6 +51,7 @@ def parse():
                     help="approximate CPU time of the oracle baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compensated", action="store_true")
     return ap.parse_args()
 
 
@@ -301,6 +302,34 @@ def run_b200(args):
     bytes_per_launch = BYTES_PER_CELL["real"] * cells
     achieved = bytes_per_launch / (ms_per_step / 1e3) / 1e9
 
+    # ---- compensated float32 variant (Delta form, 32 B/cell) ---------------
+    comp = None
+    if not args.no_compensated:
+        from lfm_b200.compensated import CompensatedEvolver
+
+        evc = CompensatedEvolver(gravity_only(N), backend=be)
+        evc.set_psi_real(E)
+        evc.set_chi(chi)
+        evc.evolve(max(args.warmup, 4))
+        evc.warm_graphs()
+        torch.cuda.synchronize(dev)
+        barrier()
+        ca = torch.cuda.Event(enable_timing=True)
+        cb = torch.cuda.Event(enable_timing=True)
+        ca.record(stream)
+        evc.evolve(args.steps)
+        cb.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        cms = max_over_ranks(ca.elapsed_time(cb)) / args.steps
+        cach = 32 * cells / (cms / 1e3) / 1e9
+        comp = {"value": world * cells / (cms / 1e3) / 1e9, "unit": METRIC, "ms_per_step": cms,
+                "bytes_per_cell": 32,
+                "roofline": {"bound": "hbm", "achieved": cach, "peak": peak, "unit": "GB/s",
+                             "frac": cach / peak, "frac_at_24B": 24 * cells / (cms / 1e3) / 1e9 / peak},
+                "tile": _lib.tune_get(0, N)}
+        del evc
+
     # ---- end to end through the public API ---------------------------------
     e2e = None
     if not args.no_e2e:
@@ -357,6 +386,8 @@ def run_b200(args):
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if comp is not None:
+        line["compensated"] = comp
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
     if world > 1:

@@ -163,6 +163,32 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
                            void* stream);
 
 /* ------------------------------------------------------------------------
+ * Compensated float32 steps (Delta form).  No counterpart kernel in the
+ * reference; they advance the same equations as lfm_leapfrog_real_f32 /
+ * _complex_f32 (numpy_backend.py:80-205) with more accuracy.
+ *
+ * State per field: the value (psi, chi) and the increment
+ * d = value - previous value as the reference stores it ((1-mask)*psi_prev
+ * for Psi, chi_prev for chi).  A step reads the values (stencil) and the
+ * increments, writes the new values to *_next (distinct buffers) and the
+ * new increments over the old ones.  The new value's rounding error is
+ * folded into its increment (two-sum), so the sub-ulp part of each update is
+ * carried forward instead of lost.  Moves 32 B/cell (REAL), 48 B (COMPLEX).
+ * ------------------------------------------------------------------------ */
+int lfm_leapfrog_real_comp_f32(const float* psi, float* psi_next, float* dpsi_io,
+                               const float* chi, float* chi_next, float* dchi_io,
+                               const float* mask_table, const lfm_mask_lut* lut, int N,
+                               double dt2, double kappa, double lambda_self, double chi0,
+                               double e0_sq, void* stream);
+
+int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* dpsi_r_io,
+                                  const float* psi_i, float* psi_i_next, float* dpsi_i_io,
+                                  const float* chi, float* chi_next, float* dchi_io,
+                                  const float* mask_table, const lfm_mask_lut* lut, int N,
+                                  double dt2, double kappa, double lambda_self, double chi0,
+                                  double e0_sq, double epsilon_w, void* stream);
+
+/* ------------------------------------------------------------------------
  * S_a Helmholtz solve (numpy_backend.py:341-356, cupy_backend.py:261-279):
  * sa_raw[a] = IRFFT[ gamma/(gamma + D|k|^2) * RFFT(|Psi_a|^2) ] for a = 0..2,
  * k = 2*pi*fftfreq(N), computed in float32 with cuFFT (R2C, hand-written

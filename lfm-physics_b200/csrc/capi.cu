@@ -518,6 +518,62 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
+int lfm_leapfrog_real_comp_f32(const float* psi, float* psi_next, float* dpsi_io,
+                               const float* chi, float* chi_next, float* dchi_io,
+                               const float* mask_table, const lfm_mask_lut* lut, int N,
+                               double dt2, double kappa, double lambda_self, double chi0,
+                               double e0_sq, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi || !psi_next || !dpsi_io || !chi || !chi_next || !dchi_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi, b}, {chi, b}},
+                      {{psi_next, b}, {dpsi_io, b}, {chi_next, b}, {dchi_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_REAL;
+  a.N = N;
+  a.comp = 1;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, 0, 0, 0, 0, 0);
+  a.pr = psi; a.pr_prev = dpsi_io; a.pr_out = psi_next; a.pr_prev_out = dpsi_io;
+  a.chi = chi; a.chi_prev = dchi_io; a.chi_out = chi_next; a.chi_prev_out = dchi_io;
+  a.lut = device_lut(mask_table, lut);
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* dpsi_r_io,
+                                  const float* psi_i, float* psi_i_next, float* dpsi_i_io,
+                                  const float* chi, float* chi_next, float* dchi_io,
+                                  const float* mask_table, const lfm_mask_lut* lut, int N,
+                                  double dt2, double kappa, double lambda_self, double chi0,
+                                  double e0_sq, double epsilon_w, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r || !psi_r_next || !dpsi_r_io || !psi_i || !psi_i_next || !dpsi_i_io || !chi ||
+      !chi_next || !dchi_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r, b}, {psi_i, b}, {chi, b}},
+                      {{psi_r_next, b}, {dpsi_r_io, b}, {psi_i_next, b}, {dpsi_i_io, b},
+                       {chi_next, b}, {dchi_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COMPLEX;
+  a.N = N;
+  a.comp = 1;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, 0, 0, 0, 0);
+  a.pr = psi_r; a.pr_prev = dpsi_r_io; a.pr_out = psi_r_next; a.pr_prev_out = dpsi_r_io;
+  a.pi = psi_i; a.pi_prev = dpsi_i_io; a.pi_out = psi_i_next; a.pi_prev_out = dpsi_i_io;
+  a.chi = chi; a.chi_prev = dchi_io; a.chi_out = chi_next; a.chi_prev_out = dchi_io;
+  a.lut = device_lut(mask_table, lut);
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
 int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
                          float* sa_raw, int N, double sa_gamma, double sa_d, void* stream) {
   int rc = check_n(N);

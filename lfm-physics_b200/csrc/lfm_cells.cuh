@@ -197,3 +197,164 @@ __device__ __forceinline__ float color_finish(const ColorAcc& A, float lapX, flo
 }
 
 }  // namespace lfm
+
+// ---- compensated float32 (Delta form) ----------------------------------------
+//
+// State per field: the value P and the increment D = P - P_prev, where
+// P_prev is the previous value as the reference stores it ((1-mask)*P for
+// Psi, undamped for chi).  The leapfrog with the sponge becomes
+//   Psi:  D' = (1-m)(D + dt2*acc),          Psi' = Psi - m*Psi + D'
+//   chi:  r  = D + dt2*acc  (clamped so that chi + r >= -chi0),
+//         D' = r + m*(chi0 - chi - r),      chi' = chi + D'
+// which is the reference update in exact arithmetic.  The new value is
+// formed with error-free transformations (two-sum, FMA two-product); its
+// rounding error is added to the stored increment, so the bits lost when
+// the small increment meets the large value come back in the next step
+// (compensated summation).  FMA is used freely: this path is measured
+// against the float64 oracle, not against the float32 reference bits.
+namespace lfm {
+
+// Rounding error of s = a + b (Knuth's two-sum): a + b == s + err exactly.
+__device__ __forceinline__ float two_sum_err(float a, float b, float s) {
+  const float bb = __fsub_rn(s, a);
+  return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// FMA-form Laplacian (same neighbours; sums then two fused weightings).
+__device__ __forceinline__ float lap19_fma(const S19& f) {
+  float faces = f.im + f.ip;
+  faces += f.jm;
+  faces += f.jp;
+  faces += f.km;
+  faces += f.kp;
+  float edges = f.imjm + f.imjp;
+  edges += f.ipjm;
+  edges += f.ipjp;
+  edges += f.imkm;
+  edges += f.imkp;
+  edges += f.ipkm;
+  edges += f.ipkp;
+  edges += f.jmkm;
+  edges += f.jmkp;
+  edges += f.jpkm;
+  edges += f.jpkp;
+  return fmaf((float)(1.0 / 3.0), faces, fmaf((float)(1.0 / 6.0), edges, -4.0f * f.c));
+}
+
+// Laplacian as weighted sums of neighbour - centre differences: the same
+// value in exact arithmetic (the weights sum to 4), but each difference of
+// two nearby values is exact in float32 (Sterbenz), so a smooth field keeps
+// its full precision -- chi ~ 19 loses nothing to the large neighbour sums.
+__device__ __forceinline__ float lap19_diff(const S19& f) {
+  const float c = f.c;
+  float faces = (f.im - c) + (f.ip - c);
+  faces += (f.jm - c) + (f.jp - c);
+  faces += (f.km - c) + (f.kp - c);
+  float edges = (f.imjm - c) + (f.imjp - c);
+  edges += (f.ipjm - c) + (f.ipjp - c);
+  edges += (f.imkm - c) + (f.imkp - c);
+  edges += (f.ipkm - c) + (f.ipkp - c);
+  edges += (f.jmkm - c) + (f.jmkp - c);
+  edges += (f.jpkm - c) + (f.jpkp - c);
+  return fmaf((float)(1.0 / 3.0), faces, (float)(1.0 / 6.0) * edges);
+}
+
+// lap - chi^2 * p with the rounding errors of chi^2 and of the product folded
+// back in (FMA two-products): the mass term is the largest one in GOV-01.
+__device__ __forceinline__ float accel_mass(float lap, float chi, float p) {
+  const float sq = __fmul_rn(chi, chi);
+  const float e_sq = fmaf(chi, chi, -sq);  // chi^2 == sq + e_sq
+  const float q = __fmul_rn(sq, p);
+  const float e_q = fmaf(sq, p, -q);       // sq*p == q + e_q
+  return (lap - q) - fmaf(e_sq, p, e_q);
+}
+
+struct CompVal {
+  float v, d;  // new value, new stored increment
+};
+
+// Psi update with the sponge: D' = (1-m)t, t = D + dt2*acc; Psi' = Psi - m*Psi + D'.
+__device__ __forceinline__ CompVal comp_psi(float psi, float d, float acc, float m,
+                                            const StepConsts& s) {
+  // The operations inside the error-free transformations are pinned with
+  // _rn intrinsics so that the compiler cannot fuse them.
+  const float t = fmaf(s.dt2, acc, d);
+  const float dn = fmaf(-m, t, t);            // (1-m)*t, one rounding
+  const float p = __fmul_rn(m, psi);
+  const float ep = fmaf(m, psi, -p);          // m*psi == p + ep
+  const float inc = __fsub_rn(dn, p);
+  const float e2 = two_sum_err(dn, -p, inc);  // dn - p == inc + e2
+  const float v = __fadd_rn(psi, inc);
+  const float e3 = two_sum_err(psi, inc, v);  // psi + inc == v + e3
+  CompVal o;
+  o.v = v;
+  o.d = dn + ((e3 + e2) - ep);                // Psi'_exact - v folded into D'
+  return o;
+}
+
+// chi update: clamp at -chi0 and the sponge blend m*chi0 + (1-m)*chi_raw in
+// increment form.
+__device__ __forceinline__ CompVal comp_chi(float chi, float d, float acc, float m,
+                                            const StepConsts& s) {
+  float r = fmaf(s.dt2, acc, d);
+  if (chi + r < s.neg_chi0) r = s.neg_chi0 - chi;
+  const float inc = fmaf(m, (s.chi0 - chi) - r, r);
+  const float v = __fadd_rn(chi, inc);
+  CompVal o;
+  o.v = v;
+  o.d = inc + two_sum_err(chi, inc, v);
+  return o;
+}
+
+__device__ __forceinline__ float comp_mexican_hat(float acc, float chi, float chi_sq,
+                                                  const StepConsts& s) {
+  if (!s.use_lambda) return acc;
+  return fmaf(-s.four_lambda * chi, chi_sq - s.chi0_sq, acc);
+}
+
+struct RealComp {
+  CompVal psi, chi;
+};
+
+__device__ __forceinline__ RealComp real_cell_comp(float lapE, float e, float de, float lapX,
+                                                   float chi, float dchi, float mask,
+                                                   const StepConsts& s) {
+  const float chi_sq = chi * chi;
+  const float accE = accel_mass(lapE, chi, e);
+  const float src = s.k_over_chi0 * chi * fmaf(e, e, -s.e0_sq);
+  float accX = lapX - src;
+  accX = comp_mexican_hat(accX, chi, chi_sq, s);
+  RealComp o;
+  o.psi = comp_psi(e, de, accE, mask, s);
+  o.chi = comp_chi(chi, dchi, accX, mask, s);
+  return o;
+}
+
+struct ComplexComp {
+  CompVal pr, pi, chi;
+};
+
+__device__ __forceinline__ ComplexComp complex_cell_comp(float lapR, float pr, float dr,
+                                                         const Faces& R, float lapI, float pi,
+                                                         float di, const Faces& I, float lapX,
+                                                         float chi, float dchi, float mask,
+                                                         const StepConsts& s) {
+  const float chi_sq = chi * chi;
+  const float accR = accel_mass(lapR, chi, pr);
+  const float accI = accel_mass(lapI, chi, pi);
+  const float psi_sq = fmaf(pr, pr, pi * pi);
+  const float jx = pr * (I.ip - I.im) - pi * (R.ip - R.im);
+  const float jy = pr * (I.jp - I.jm) - pi * (R.jp - R.jm);
+  const float jz = pr * (I.kp - I.km) - pi * (R.kp - R.km);
+  const float jt = 0.5f * (jx + jy + jz);
+  const float src = s.k_over_chi0 * chi * (fmaf(s.eps_w, jt, psi_sq) - s.e0_sq);
+  float accX = lapX - src;
+  accX = comp_mexican_hat(accX, chi, chi_sq, s);
+  ComplexComp o;
+  o.pr = comp_psi(pr, dr, accR, mask, s);
+  o.pi = comp_psi(pi, di, accI, mask, s);
+  o.chi = comp_chi(chi, dchi, accX, mask, s);
+  return o;
+}
+
+}  // namespace lfm

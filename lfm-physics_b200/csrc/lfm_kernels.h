@@ -33,6 +33,7 @@ struct StepArgs {
   const float* sa;     // raw S_a (3*N^3) or null
   float* sa_clip_out;  // clipped S_a copy (protocol colour step) or null
   int damp_prev;       // multiply the previous-step fields by (1-mask) on read
+  int comp;            // compensated Delta form: *_prev hold increments, updated in place
   int* status;         // device status word for bounded waits
 };
 

@@ -82,6 +82,31 @@ __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
     const float absorb = fsub(1.0f, mask);
     const S19 X = gather(a.chi, ix);
     const float chi_prev = a.chi_prev[x];
+    if (LEVEL != LFM_COLOR && a.comp) {
+      // compensated Delta form: *_prev hold the increments (updated in place)
+      if (LEVEL == LFM_REAL) {
+        const S19 E = gather(a.pr, ix);
+        const RealComp o = real_cell_comp(lap19_fma(E), E.c, a.pr_prev[x], lap19_diff(X), X.c,
+                                          chi_prev, mask, a.c);
+        a.pr_out[x] = o.psi.v;
+        a.pr_prev_out[x] = o.psi.d;
+        a.chi_out[x] = o.chi.v;
+        a.chi_prev_out[x] = o.chi.d;
+      } else {
+        const S19 R = gather(a.pr, ix);
+        const S19 I = gather(a.pi, ix);
+        const ComplexComp o = complex_cell_comp(lap19_fma(R), R.c, a.pr_prev[x], faces_of(R),
+                                                lap19_fma(I), I.c, a.pi_prev[x], faces_of(I),
+                                                lap19_diff(X), X.c, chi_prev, mask, a.c);
+        a.pr_out[x] = o.pr.v;
+        a.pr_prev_out[x] = o.pr.d;
+        a.pi_out[x] = o.pi.v;
+        a.pi_prev_out[x] = o.pi.d;
+        a.chi_out[x] = o.chi.v;
+        a.chi_prev_out[x] = o.chi.d;
+      }
+      continue;
+    }
     if (LEVEL == LFM_REAL) {
       const S19 E = gather(a.pr, ix);
       const RealOut o =

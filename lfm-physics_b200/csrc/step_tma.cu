@@ -570,7 +570,7 @@ struct QShared {
 // the centre plane's stage when it is done with it, and the last warp to do
 // so refills the stage with the plane S further on.  Returns false when the
 // CTA must stop (a bounded wait gave up).
-template <int LEVEL, int V, int PA, int PB, int PC>
+template <int LEVEL, int V, bool COMP, int PA, int PB, int PC>
 __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
                                         const QLane& L, int c, int i0, int i1, int j0,
@@ -609,7 +609,49 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
 #pragma unroll
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
   const int64_t gofs = ((int64_t)i * N + j) * N + k0;
-  if constexpr (LEVEL == LFM_REAL) {
+  if constexpr (COMP) {
+    // Delta form: point fields hold the increments; new values go to the
+    // *_out buffers, new increments over the increments (*_prev_out).
+    if constexpr (LEVEL == LFM_REAL) {
+      const Vec<V> de = lds<V>(smem, bc + L.o_pt);
+      const Vec<V> dx = lds<V>(smem, bc + L.o_pt + PTS);
+      float o_e[V], o_de[V], o_x[V], o_dx[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const S19 E = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 X = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const RealComp o =
+            real_cell_comp(lap19_fma(E), E.c, de.v[e], lap19_diff(X), X.c, dx.v[e], mask[e], a.c);
+        o_e[e] = o.psi.v; o_de[e] = o.psi.d; o_x[e] = o.chi.v; o_dx[e] = o.chi.d;
+      }
+      stg<V>(a.pr_out + gofs, o_e);
+      stg<V>(a.pr_prev_out + gofs, o_de);
+      stg<V>(a.chi_out + gofs, o_x);
+      stg<V>(a.chi_prev_out + gofs, o_dx);
+    } else {
+      const Vec<V> dr = lds<V>(smem, bc + L.o_pt);
+      const Vec<V> di = lds<V>(smem, bc + L.o_pt + PTS);
+      const Vec<V> dx = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+      float o_r[V], o_dr[V], o_i[V], o_di[V], o_x[V], o_dx[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const S19 R = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 I = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const S19 X = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
+        const ComplexComp o = complex_cell_comp(lap19_fma(R), R.c, dr.v[e], faces_of(R),
+                                                lap19_fma(I), I.c, di.v[e], faces_of(I),
+                                                lap19_diff(X), X.c, dx.v[e], mask[e], a.c);
+        o_r[e] = o.pr.v; o_dr[e] = o.pr.d; o_i[e] = o.pi.v; o_di[e] = o.pi.d;
+        o_x[e] = o.chi.v; o_dx[e] = o.chi.d;
+      }
+      stg<V>(a.pr_out + gofs, o_r);
+      stg<V>(a.pr_prev_out + gofs, o_dr);
+      stg<V>(a.pi_out + gofs, o_i);
+      stg<V>(a.pi_prev_out + gofs, o_di);
+      stg<V>(a.chi_out + gofs, o_x);
+      stg<V>(a.chi_prev_out + gofs, o_dx);
+    }
+  } else if constexpr (LEVEL == LFM_REAL) {
     const Vec<V> ep = lds<V>(smem, bc + L.o_pt);
     const Vec<V> xp = lds<V>(smem, bc + L.o_pt + PTS);
     float o_psi[V], o_chi[V], o_pp[V], o_cp[V];
@@ -670,7 +712,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   return true;
 }
 
-template <int LEVEL, int V>
+template <int LEVEL, int V, bool COMP>
 __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
   constexpr int NS = QFields<LEVEL>::ns;
   extern __shared__ __align__(128) float smem[];
@@ -750,13 +792,13 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
     uint32_t ph_nxt = (uint32_t)((2 / S) & 1);
     int c = 0;
     while (true) {
-      if (c >= n || !q_plane<LEVEL, V, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes,
+      if (c >= n || !q_plane<LEVEL, V, COMP, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes,
                                                 nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+      if (++c >= n || !q_plane<LEVEL, V, COMP, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
                                                   nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+      if (++c >= n || !q_plane<LEVEL, V, COMP, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
                                                   nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
         break;
       ++c;
@@ -890,25 +932,25 @@ cudaError_t launch_kernel(K kernel, int* granted, std::mutex* mu, const TmaParam
   return cudaGetLastError();
 }
 
-template <int LEVEL, int V, bool QUEUE>
+template <int LEVEL, int V, bool QUEUE, bool COMP>
 struct KernelSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
     if constexpr (QUEUE)
-      return tma_queue_kernel<LEVEL, V>;
+      return tma_queue_kernel<LEVEL, V, COMP>;
     else
       return tma_step_kernel<LEVEL, V>;
   }
 };
-template <int LEVEL, int V, bool QUEUE>
-std::mutex KernelSlot<LEVEL, V, QUEUE>::mu;
-template <int LEVEL, int V, bool QUEUE>
-int KernelSlot<LEVEL, V, QUEUE>::granted = 0;
+template <int LEVEL, int V, bool QUEUE, bool COMP>
+std::mutex KernelSlot<LEVEL, V, QUEUE, COMP>::mu;
+template <int LEVEL, int V, bool QUEUE, bool COMP>
+int KernelSlot<LEVEL, V, QUEUE, COMP>::granted = 0;
 
-template <int LEVEL, int V, bool QUEUE>
+template <int LEVEL, int V, bool QUEUE, bool COMP = false>
 cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t stream) {
-  using Slot = KernelSlot<LEVEL, V, QUEUE>;
+  using Slot = KernelSlot<LEVEL, V, QUEUE, COMP>;
   int regs = 0;
   cudaError_t e = kernel_regs(Slot::fn(), &regs);
   if (e != cudaSuccess) return e;
@@ -985,6 +1027,16 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   TileConfig forced_cfg;
   const bool have_forced = tune_lookup(a.level, N, &forced_cfg);
   const TileConfig* forced = have_forced ? &forced_cfg : nullptr;
+  if (a.comp) {
+    // compensated Delta form: REAL and COMPLEX, register-queue kernel only
+    if (a.level == LFM_REAL)
+      return (N % 4) ? cudaErrorNotSupported
+                     : plan_and_launch<LFM_REAL, 4, true, true>(P, forced, stream);
+    if (a.level == LFM_COMPLEX)
+      return (N % 2) ? cudaErrorNotSupported
+                     : plan_and_launch<LFM_COMPLEX, 2, true, true>(P, forced, stream);
+    return cudaErrorNotSupported;
+  }
   if (a.level == LFM_REAL) {
     const int v = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 4;
     if (N % v) return cudaErrorNotSupported;
