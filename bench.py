@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compensated", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-lattices", type=int, default=256)
+    ap.add_argument("--batch-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -237,6 +240,86 @@ def run_reference(args):
     return 0
 
 
+def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
+    """Batched sweep: `batch_lattices` lattices (N in {32..96}, REAL/COMPLEX mixed,
+    one packet each) in one persistent launch per level and step, the whole
+    step loop replayed as one CUDA graph, against the plain loop of
+    single-lattice Evolvers over the same lattices on the same GPU."""
+    import torch
+
+    from lfm_b200 import Evolver, _lib
+    from lfm_b200.batch import BatchedLattices
+    from lfm_b200.workloads import sweep_lattices
+
+    steps = args.batch_steps + (args.batch_steps % 2)
+    L = sweep_lattices(args.batch_lattices, seed=5 + 1000 * rank)
+    cfgs = [c for c, _, _ in L]
+    cells = sum(c.grid_size**3 for c in cfgs)
+    bytes_step = sum(c.grid_size**3 * (36 if int(c.field_level) else 24) for c in cfgs)
+    stream = torch.cuda.current_stream(dev)
+
+    def load(tgt, i, pr, pi):
+        args_ = (i,) if isinstance(tgt, BatchedLattices) else ()
+        tgt.set_psi_real(*args_, pr)
+        if pi is not None:
+            tgt.set_psi_imag(*args_, pi)
+
+    def timed(fn):
+        torch.cuda.synchronize(dev)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return max_over_ranks(a.elapsed_time(b))
+
+    B = BatchedLattices(cfgs, backend=be)
+    B.graph_block = steps
+    for i, (c, pr, pi) in enumerate(L):
+        load(B, i, pr, pi)
+    B.evolve(max(args.warmup, 3) | 1)  # odd: leaves the damped state, parity 1
+    B.evolve(steps)                    # captures the whole-loop graph of this parity
+    B.evolve(steps)                    # ... and of the other
+    ms_b = timed(lambda: B.evolve(steps))
+    status = _lib.device_status(clear=True)
+    if status:
+        raise RuntimeError(f"device status word {status} after the batched steps")
+    info = B.info()
+    del B
+
+    evs = []
+    for c, pr, pi in L:
+        ev = Evolver(c, backend=be)
+        load(ev, 0, pr, pi)
+        ev.evolve(max(args.warmup, 3) | 1)
+        ev.warm_graphs()
+        evs.append(ev)
+
+    def plain():
+        for ev in evs:
+            ev.evolve(steps)
+
+    ms_p = timed(plain)
+    del evs
+    vb = cells * steps / (ms_b / 1e3) / 1e9
+    vp = cells * steps / (ms_p / 1e3) / 1e9
+    ach = bytes_step * steps / (ms_b / 1e3) / 1e9
+    return {"value": vb, "unit": METRIC, "ms": ms_b, "steps": steps,
+            "lattices": len(cfgs), "cells": cells,
+            "levels": {"real": sum(1 for c in cfgs if int(c.field_level) == 0),
+                       "complex": sum(1 for c in cfgs if int(c.field_level) == 1)},
+            "plain_loop": {"value": vp, "unit": METRIC, "ms": ms_p,
+                           "how": "one Evolver per lattice, evolve(steps) each in turn "
+                                  "(two-step CUDA graphs)"},
+            "speedup_vs_plain_loop": ms_p / ms_b,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "bytes_per_cell": "24 REAL / 36 COMPLEX"},
+            "launch": info, "gpu_launches": 2 * steps}
+
+
 def run_b200(args):
     import numpy as np
     import torch
@@ -330,6 +413,10 @@ def run_b200(args):
                 "tile": _lib.tune_get(0, N)}
         del evc
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, be, dev, rank, barrier, max_over_ranks, peak)
+
     # ---- end to end through the public API ---------------------------------
     e2e = None
     if not args.no_e2e:
@@ -388,6 +475,8 @@ def run_b200(args):
         line["e2e"] = e2e
     if comp is not None:
         line["compensated"] = comp
+    if batched is not None:
+        line["batched"] = batched
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
     if world > 1:

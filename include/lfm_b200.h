@@ -189,6 +189,56 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
                                   double e0_sq, double epsilon_w, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Batches of independent lattices (the runs lfm/sweep.py:14-157 makes one
+ * Simulation at a time), stepped together: one launch per field level and
+ * step, persistent CTAs walking a static work list of (lattice, row tile,
+ * plane chunk) items sorted by cost, each item marched like the fused
+ * single-lattice kernel.  REAL and COMPLEX lattices, N a multiple of 4, any
+ * mix of sizes and parameters.  Each lattice keeps two slots per field in
+ * the resident layout of lfm_leapfrog_*_f32: at parity p, slot p holds the
+ * current fields and slot 1-p the previous ones, which the step overwrites
+ * with the new fields.  damp_prev as in lfm_leapfrog_*_f32.
+ * ------------------------------------------------------------------------ */
+typedef struct lfm_lattice_desc {
+  int32_t N;
+  int32_t level;          /* LFM_REAL or LFM_COMPLEX */
+  float* psi_r[2];        /* slots of Psi (real part) */
+  float* psi_i[2];        /* slots of the imaginary part; NULL at the REAL level */
+  float* chi[2];          /* slots of chi */
+  const float* mask_table;
+  lfm_mask_lut lut;
+  double dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w;
+} lfm_lattice_desc;
+
+typedef struct lfm_batch_tuning {
+  int32_t threads;      /* cap on the CTA size (multiple of 32, <= 512); 0 = 256 */
+  int32_t stages;       /* shared-memory stages, 3..6; 0 = 3 */
+  int32_t item_cells;   /* target cells per work item; 0 = 65536 */
+  int32_t ctas_per_sm;  /* persistent CTAs per SM; 0 = as many as fit */
+} lfm_batch_tuning;
+
+typedef struct lfm_batch lfm_batch;
+
+/* Plans the work lists and uploads the descriptors (device memory owned by
+ * the batch).  tuning may be NULL.  The buffers stay owned by the caller. */
+int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
+                     const lfm_batch_tuning* tuning, lfm_batch** out);
+/* One step of every lattice: at most two launches (REAL, then COMPLEX). */
+int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream);
+/* Launch shape of one level's kernel (items = 0 when the batch has no lattice of it). */
+int lfm_batch_info(const lfm_batch* batch, int level, int* items, int* threads, int* grid,
+                   int* smem);
+int lfm_batch_destroy(lfm_batch* batch);
+/* The plan lfm_batch_create would make, on the host only (no device needed;
+ * 128 registers per thread and `sms` SMs assumed, 148 when sms <= 0).
+ * items_out: 6 int32 per item (level, lattice, j0, j1, i0, i1), REAL items
+ * first, each level in launch order; launch_out: (threads, smem, grid) per
+ * level.  Either may be NULL; nitems_out gets the item count. */
+int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_tuning* tuning,
+                   int sms, int32_t* items_out, int max_items, int* nitems_out,
+                   int32_t* launch_out);
+
+/* ------------------------------------------------------------------------
  * S_a Helmholtz solve (numpy_backend.py:341-356, cupy_backend.py:261-279):
  * sa_raw[a] = IRFFT[ gamma/(gamma + D|k|^2) * RFFT(|Psi_a|^2) ] for a = 0..2,
  * k = 2*pi*fftfreq(N), computed in float32 with cuFFT (R2C, hand-written

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "lfm_b200.h"
+#include "lfm_batch.h"
 #include "lfm_kernels.h"
 #include "lfm_metrics.h"
 
@@ -717,6 +718,290 @@ int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(e, "metrics readback");
   finish_metrics(r, a.chi_shift, out_host);
+  return LFM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batches of lattices
+// ---------------------------------------------------------------------------
+namespace {
+
+// Host-side plan of a batch: tile shape per lattice, one work list and one
+// launch shape per level.  Pure host arithmetic (lfm_batch_plan exposes it
+// without a device).
+struct BatchPlan {
+  struct Level {
+    std::vector<lfm::BatchItem> items;
+    int threads = 0, smem = 0, grid = 0;
+  } lv[2];  // REAL, COMPLEX
+  std::vector<int> TJ, IC, stage_floats;
+};
+
+constexpr int kBatchSmemLimit = 226 * 1024;
+
+int validate_batch_tuning(const lfm_batch_tuning* in, lfm_batch_tuning* t) {
+  *t = lfm_batch_tuning{256, 3, 65536, 0};
+  if (in) {
+    if (in->threads) t->threads = in->threads;
+    if (in->stages) t->stages = in->stages;
+    if (in->item_cells) t->item_cells = in->item_cells;
+    t->ctas_per_sm = in->ctas_per_sm;
+  }
+  if (t->threads < 32 || t->threads > 512 || t->threads % 32)
+    return fail(LFM_ERR_INVALID_ARG, "threads %d not a multiple of 32 in [32, 512]", t->threads);
+  if (t->stages < 3 || t->stages > 6) return fail(LFM_ERR_INVALID_ARG, "stages %d not in [3, 6]", t->stages);
+  if (t->item_cells < 1024) return fail(LFM_ERR_INVALID_ARG, "item_cells %d < 1024", t->item_cells);
+  if (t->ctas_per_sm < 0) return fail(LFM_ERR_INVALID_ARG, "ctas_per_sm %d", t->ctas_per_sm);
+  return LFM_OK;
+}
+
+int check_lattice_shape(const lfm_lattice_desc& d, int l) {
+  int rc = check_n(d.N);
+  if (rc) return rc;
+  if (d.level != LFM_REAL && d.level != LFM_COMPLEX)
+    return fail(LFM_ERR_UNSUPPORTED, "lattice %d: level %d (batches hold REAL and COMPLEX)", l,
+                d.level);
+  if (d.N % 4 || d.N < 8)
+    return fail(LFM_ERR_UNSUPPORTED, "lattice %d: N=%d is not a multiple of 4 >= 8", l, d.N);
+  return LFM_OK;
+}
+
+// regs[level]: registers per thread of the batch kernel; sms: SM count.
+int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t,
+               const int regs[2], int sms, BatchPlan* plan) {
+  plan->TJ.assign(count, 0);
+  plan->IC.assign(count, 0);
+  plan->stage_floats.assign(count, 0);
+  for (int level = 0; level < 2; ++level) {
+    BatchPlan::Level& out = plan->lv[level];
+    const int V = (level == LFM_REAL) ? 4 : 2;
+    const int ns = (level == LFM_REAL) ? 2 : 3;
+    int threads = 32, max_stage = 0;
+    for (int l = 0; l < count; ++l) {
+      if (L[l].level != level) continue;
+      const int N = L[l].N;
+      const int tpr = N / V;
+      if (tpr > t.threads)
+        return fail(LFM_ERR_UNSUPPORTED, "lattice %d: a row of N=%d needs %d threads > %d", l, N,
+                    tpr, t.threads);
+      int TJ = 1;
+      for (int d = 1; d <= N; ++d)
+        if (N % d == 0 && d * tpr <= t.threads) TJ = d;
+      // chunks of about item_cells cells, the planes split as evenly as possible
+      const double cells = (double)TJ * N * N;
+      const int chunks = std::max(1, std::min(N / 2, (int)(cells / t.item_cells + 0.5)));
+      const int IC = (N + chunks - 1) / chunks;
+      plan->TJ[l] = TJ;
+      plan->IC[l] = IC;
+      // ns halo-extended fields + ns point fields (the previous-step values)
+      plan->stage_floats[l] = N * (ns * (TJ + 2) + ns * TJ);
+      max_stage = std::max(max_stage, plan->stage_floats[l]);
+      threads = std::max(threads, ((TJ * tpr + 31) / 32) * 32);
+      for (int j0 = 0; j0 < N; j0 += TJ)
+        for (int i0 = 0; i0 < N; i0 += IC) out.items.push_back({l, j0, i0, std::min(N, i0 + IC)});
+    }
+    if (out.items.empty()) continue;
+    // largest items first: the static stride then spreads the cost evenly
+    std::stable_sort(out.items.begin(), out.items.end(),
+                     [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
+                       const long ca = (long)plan->TJ[a.lattice] * L[a.lattice].N * (a.i1 - a.i0);
+                       const long cb = (long)plan->TJ[b.lattice] * L[b.lattice].N * (b.i1 - b.i0);
+                       return ca > cb;
+                     });
+    out.threads = threads;
+    out.smem = t.stages * max_stage * (int)sizeof(float);
+    if (out.smem > kBatchSmemLimit)
+      return fail(LFM_ERR_UNSUPPORTED, "batch needs %d B of shared memory per CTA (limit %d)",
+                  out.smem, kBatchSmemLimit);
+    int per_sm = std::min({(228 * 1024) / (out.smem + 1024), 2048 / threads,
+                           65536 / std::max(1, regs[level] * threads)});
+    per_sm = std::max(1, per_sm);
+    if (t.ctas_per_sm > 0) per_sm = std::min(per_sm, t.ctas_per_sm);
+    out.grid = std::min((int)out.items.size(), sms * per_sm);
+  }
+  return LFM_OK;
+}
+
+}  // namespace
+
+struct lfm_batch {
+  int device = 0;
+  int stages = 3;
+  lfm::BatchLattice* d_lat = nullptr;
+  struct Level {
+    lfm::BatchItem* d_items = nullptr;
+    int nitems = 0, threads = 0, smem = 0, grid = 0;
+  } lv[2];
+};
+
+extern "C" {
+
+int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_tuning* tuning,
+                   int sms, int32_t* items_out, int max_items, int* nitems_out,
+                   int32_t* launch_out) {
+  if (!lattices || count <= 0) return fail(LFM_ERR_INVALID_ARG, "empty batch");
+  lfm_batch_tuning t;
+  int rc = validate_batch_tuning(tuning, &t);
+  if (rc) return rc;
+  for (int l = 0; l < count; ++l) {
+    rc = check_lattice_shape(lattices[l], l);
+    if (rc) return rc;
+  }
+  const int regs[2] = {128, 128};
+  BatchPlan plan;
+  rc = plan_batch(lattices, count, t, regs, sms > 0 ? sms : 148, &plan);
+  if (rc) return rc;
+  const int total = (int)(plan.lv[0].items.size() + plan.lv[1].items.size());
+  if (nitems_out) *nitems_out = total;
+  if (items_out) {
+    if (max_items < total) return fail(LFM_ERR_CAPACITY, "%d items > capacity %d", total, max_items);
+    int k = 0;
+    for (int lv = 0; lv < 2; ++lv)
+      for (const lfm::BatchItem& it : plan.lv[lv].items) {
+        items_out[6 * k + 0] = lv;
+        items_out[6 * k + 1] = it.lattice;
+        items_out[6 * k + 2] = it.j0;
+        items_out[6 * k + 3] = it.j0 + plan.TJ[it.lattice];
+        items_out[6 * k + 4] = it.i0;
+        items_out[6 * k + 5] = it.i1;
+        ++k;
+      }
+  }
+  if (launch_out)
+    for (int lv = 0; lv < 2; ++lv) {
+      launch_out[3 * lv + 0] = plan.lv[lv].threads;
+      launch_out[3 * lv + 1] = plan.lv[lv].smem;
+      launch_out[3 * lv + 2] = plan.lv[lv].grid;
+    }
+  return LFM_OK;
+}
+
+int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
+                     const lfm_batch_tuning* tuning, lfm_batch** out) {
+  if (!lattices || count <= 0 || !out) return fail(LFM_ERR_INVALID_ARG, "empty batch");
+  lfm_batch_tuning t;
+  int rc = validate_batch_tuning(tuning, &t);
+  if (rc) return rc;
+  int* status = nullptr;
+  rc = status_word(&status);
+  if (rc) return rc;
+  std::vector<lfm::BatchLattice> dev(count);
+  for (int l = 0; l < count; ++l) {
+    const lfm_lattice_desc& d = lattices[l];
+    rc = check_lattice_shape(d, l);
+    if (rc) return rc;
+    rc = check_lut(d.mask_table, &d.lut, d.N);
+    if (rc) return rc;
+    const bool cx = d.level == LFM_COMPLEX;
+    const float* ptrs[] = {d.psi_r[0], d.psi_r[1], d.chi[0], d.chi[1], cx ? d.psi_i[0] : d.chi[0],
+                           cx ? d.psi_i[1] : d.chi[1]};
+    for (const float* p : ptrs) {
+      if (!p) return fail(LFM_ERR_INVALID_ARG, "lattice %d: null slot", l);
+      if (!aligned16(p)) return fail(LFM_ERR_ALIGNMENT, "lattice %d: slot not 16-byte aligned", l);
+    }
+    lfm::BatchLattice& b = dev[l];
+    b.N = d.N;
+    b.level = d.level;
+    for (int s = 0; s < 2; ++s) {
+      b.pr[s] = d.psi_r[s];
+      b.pi[s] = cx ? d.psi_i[s] : nullptr;
+      b.chi[s] = d.chi[s];
+    }
+    b.c = lfm::make_step_consts(d.dt2, d.kappa, d.lambda_self, d.chi0, d.e0_sq, d.epsilon_w, 0,
+                                0, 0, 0);
+    b.lut = device_lut(d.mask_table, &d.lut);
+  }
+  int regs[2] = {128, 128};
+  for (int lv = 0; lv < 2; ++lv) {
+    cudaError_t e = lfm::batch_kernel_regs(lv, &regs[lv]);
+    if (e != cudaSuccess) return cuda_fail(e, "batch kernel attributes");
+  }
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  BatchPlan plan;
+  rc = plan_batch(lattices, count, t, regs, sms, &plan);
+  if (rc) return rc;
+  for (int l = 0; l < count; ++l) {
+    dev[l].TJ = plan.TJ[l];
+    dev[l].IC = plan.IC[l];
+    dev[l].stage_floats = plan.stage_floats[l];
+  }
+  lfm_batch* B = new lfm_batch;
+  B->device = device;
+  B->stages = t.stages;
+  cudaError_t e = cudaMalloc(&B->d_lat, sizeof(lfm::BatchLattice) * count);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(B->d_lat, dev.data(), sizeof(lfm::BatchLattice) * count,
+                   cudaMemcpyHostToDevice);
+  for (int lv = 0; lv < 2 && e == cudaSuccess; ++lv) {
+    const std::vector<lfm::BatchItem>& items = plan.lv[lv].items;
+    B->lv[lv].nitems = (int)items.size();
+    B->lv[lv].threads = plan.lv[lv].threads;
+    B->lv[lv].smem = plan.lv[lv].smem;
+    B->lv[lv].grid = plan.lv[lv].grid;
+    if (items.empty()) continue;
+    e = cudaMalloc(&B->lv[lv].d_items, sizeof(lfm::BatchItem) * items.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(B->lv[lv].d_items, items.data(), sizeof(lfm::BatchItem) * items.size(),
+                     cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    lfm_batch_destroy(B);
+    return cuda_fail(e, "batch descriptors");
+  }
+  *out = B;
+  return LFM_OK;
+}
+
+int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
+  if (!batch) return fail(LFM_ERR_INVALID_ARG, "null batch");
+  if (parity != 0 && parity != 1) return fail(LFM_ERR_INVALID_ARG, "parity %d", parity);
+  int* status = nullptr;
+  int rc = status_word(&status);
+  if (rc) return rc;
+  for (int lv = 0; lv < 2; ++lv) {
+    const lfm_batch::Level& L = batch->lv[lv];
+    if (!L.nitems) continue;
+    lfm::BatchParams P{};
+    P.lattices = batch->d_lat;
+    P.items = L.d_items;
+    P.nitems = L.nitems;
+    P.parity = parity;
+    P.damp_prev = damp_prev ? 1 : 0;
+    P.stages = batch->stages;
+    P.status = status;
+    cudaError_t e = lfm::launch_batch_step(lv, P, L.threads, L.smem, L.grid,
+                                           static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "batch step launch");
+  }
+  return LFM_OK;
+}
+
+int lfm_batch_info(const lfm_batch* batch, int level, int* items, int* threads, int* grid,
+                   int* smem) {
+  if (!batch) return fail(LFM_ERR_INVALID_ARG, "null batch");
+  if (level != LFM_REAL && level != LFM_COMPLEX) return fail(LFM_ERR_INVALID_ARG, "level %d", level);
+  const lfm_batch::Level& L = batch->lv[level];
+  if (items) *items = L.nitems;
+  if (threads) *threads = L.threads;
+  if (grid) *grid = L.grid;
+  if (smem) *smem = L.smem;
+  return LFM_OK;
+}
+
+int lfm_batch_destroy(lfm_batch* batch) {
+  if (!batch) return LFM_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(batch->device);
+  if (batch->d_lat) cudaFree(batch->d_lat);
+  for (auto& L : batch->lv)
+    if (L.d_items) cudaFree(L.d_items);
+  cudaSetDevice(prev);
+  delete batch;
   return LFM_OK;
 }
 

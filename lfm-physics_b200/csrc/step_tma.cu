@@ -27,6 +27,7 @@
 #include <mutex>
 
 #include "lfm_cells.cuh"
+#include "lfm_batch.h"
 #include "lfm_kernels.h"
 #include "lfm_tune.h"
 
@@ -60,6 +61,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
                : "memory");
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_init_fence() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -575,7 +579,8 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
                                         QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
                                         const QLane& L, int c, int i0, int i1, int j0,
                                         int nplanes, int nwarps, int& s_cur, int& s_nxt,
-                                        uint32_t& ph_nxt, int32_t qj, const int32_t (&qk)[V]) {
+                                        uint32_t& ph_nxt, int32_t qj, const int32_t (&qk)[V],
+                                        bool active) {
   constexpr int NS = QFields<LEVEL>::ns;
   const StepArgs& a = P.a;
   const int N = P.N, TJ = P.TJ;
@@ -589,6 +594,9 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     return false;
   }
   const int bn = s_nxt * SF, bc = s_cur * SF;
+  // Threads beyond the tile's rows (a batch tile narrower than the CTA) only
+  // take part in the waits and the stage release.
+  if (active) {
 #pragma unroll
   for (int f = 0; f < NS; ++f) {
     q_load<V>(Q[f][PC], smem, bn + f * FB, L);
@@ -691,6 +699,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     if (a.pi_prev_out) stg<V>(a.pi_prev_out + gofs, o_ip);
     if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
   }
+  }  // active
   // Release the centre plane's stage (u = c+1); the last warp refills it
   // with u = c+1+S.
   __syncwarp();
@@ -712,25 +721,22 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   return true;
 }
 
+// The march of one tile: rows j0 .. j0+rows-1 (all k), planes [i0, i1).
+// Initialises the stage barriers and the bookkeeping itself, so a CTA may
+// run several marches one after another (the batch kernel).
 template <int LEVEL, int V, bool COMP>
-__global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
+__device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_t* bars,
+                                        QShared& sh, int j0, int i0, int i1, int rows) {
   constexpr int NS = QFields<LEVEL>::ns;
-  extern __shared__ __align__(128) float smem[];
-  __shared__ __align__(8) uint64_t bars[kMaxStages];
-  __shared__ QShared sh;
-
   const int N = P.N, TJ = P.TJ, S = P.S;
-  const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
-  const int j0 = jt * TJ;
-  const int i0 = ch * P.IC;
-  const int i1 = min(i0 + P.IC, N);
   const int n = i1 - i0;
   const int nplanes = n + 2;
   const int tid = threadIdx.x;
   const int nwarps = blockDim.x >> 5;
   const int tpr = N / V;
-  const int r = tid / tpr;
-  const int k0 = (tid % tpr) * V;
+  const bool active = tid < rows * tpr;
+  const int r = active ? tid / tpr : 0;
+  const int k0 = active ? (tid % tpr) * V : 0;
   const int km1 = (k0 == 0) ? N - 1 : k0 - 1;
   const int kpv = (k0 + V == N) ? 0 : k0 + V;
   QLane L;
@@ -751,6 +757,7 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
 #pragma unroll
   for (int e = 0; e < V; ++e) qk[e] = qterm(k0 + e, N);
 
+  __syncthreads();  // a previous march in this CTA is over in every warp
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&bars[s], 1);
@@ -773,7 +780,7 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
   if (!ok) {
     sh.abort_flag = 1;
     atomicOr(P.a.status, LFM_ERR_DEVICE_TIMEOUT);
-  } else {
+  } else if (active) {
 #pragma unroll
     for (int f = 0; f < NS; ++f) {
       q_load<V>(Q[f][0], smem, 0 * P.stage_floats + f * (TJ + 2) * N, L);
@@ -792,24 +799,103 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
     uint32_t ph_nxt = (uint32_t)((2 / S) & 1);
     int c = 0;
     while (true) {
-      if (c >= n || !q_plane<LEVEL, V, COMP, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes,
-                                                nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+      if (c >= n || !q_plane<LEVEL, V, COMP, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+                                                      nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj,
+                                                      qk, active))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
-                                                  nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+                                                        nplanes, nwarps, s_cur, s_nxt, ph_nxt,
+                                                        qj, qk, active))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
-                                                  nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj, qk))
+                                                        nplanes, nwarps, s_cur, s_nxt, ph_nxt,
+                                                        qj, qk, active))
         break;
       ++c;
     }
   }
   if (*(volatile int*)&sh.abort_flag && (tid & 31) == 0) {
     // The last use of each stage is the only one that can still be in flight;
-    // let it land before this CTA's shared memory goes away.
+    // let it land before this CTA's shared memory is reused or released.
     const int issued = *(volatile int*)&sh.issued;
     for (int u = max(0, issued - S); u < issued; ++u)
       mbar_wait_bounded(&bars[u % S], (uint32_t)((u / S) & 1), kDrainLimitNs);
+  }
+}
+
+template <int LEVEL, int V, bool COMP>
+__global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
+  extern __shared__ __align__(128) float smem[];
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  __shared__ QShared sh;
+  const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
+  const int i0 = ch * P.IC;
+  q_march<LEVEL, V, COMP>(P, smem, bars, sh, jt * P.TJ, i0, min(i0 + P.IC, P.N), P.TJ);
+}
+
+// ---- batch kernel: many lattices, one launch per level and step ---------------
+//
+// Persistent CTAs walk a static work list of (lattice, row tile, plane chunk)
+// items, sorted by cost, and run the same barrier-free march on each.  The
+// per-item parameters (slot pointers for this step's parity, constants, mask
+// table, tile shape) are built in shared memory from the lattice descriptor.
+template <int LEVEL, int V>
+__global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ BatchParams B) {
+  extern __shared__ __align__(128) float smem[];
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  __shared__ QShared sh;
+  __shared__ TmaParams P;
+  for (int w = blockIdx.x; w < B.nitems; w += gridDim.x) {
+    const BatchItem it = B.items[w];
+    __syncthreads();  // every warp is done with the previous item's parameters
+    if (threadIdx.x == 0) {
+      const BatchLattice& L = B.lattices[it.lattice];
+      const int cur = B.parity, nxt = 1 - B.parity;
+      StepArgs a{};
+      a.level = LEVEL;
+      a.N = L.N;
+      a.c = L.c;
+      a.pr = L.pr[cur];
+      a.pr_prev = L.pr[nxt];
+      a.pr_out = L.pr[nxt];
+      a.chi = L.chi[cur];
+      a.chi_prev = L.chi[nxt];
+      a.chi_out = L.chi[nxt];
+      if (LEVEL == LFM_COMPLEX) {
+        a.pi = L.pi[cur];
+        a.pi_prev = L.pi[nxt];
+        a.pi_out = L.pi[nxt];
+      }
+      a.lut = L.lut;
+      a.damp_prev = B.damp_prev;
+      a.status = B.status;
+      P.a = a;
+      if (LEVEL == LFM_REAL) {
+        P.ns = 2;
+        P.sf[0] = a.pr; P.sf[1] = a.chi;
+        P.np = 2;
+        P.pf[0] = a.pr_prev; P.pf[1] = a.chi_prev;
+      } else {
+        P.ns = 3;
+        P.sf[0] = a.pr; P.sf[1] = a.pi; P.sf[2] = a.chi;
+        P.np = 3;
+        P.pf[0] = a.pr_prev; P.pf[1] = a.pi_prev; P.pf[2] = a.chi_prev;
+      }
+      P.pf_mask = -1;
+      P.pf_sa = -1;
+      P.N = L.N;
+      P.TJ = L.TJ;
+      P.IC = L.IC;
+      P.S = B.stages;
+      P.JT = L.N / L.TJ;
+      P.stage_floats = L.stage_floats;
+    }
+    __syncthreads();  // P is visible to every thread
+    q_march<LEVEL, V, false>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
+    __syncthreads();  // every wait of the march is over
+    if (sh.abort_flag) break;  // same value in every thread
+    if (threadIdx.x == 0)
+      for (int s = 0; s < P.S; ++s) mbar_inval(&bars[s]);  // re-initialised by the next march
   }
 }
 
@@ -1050,6 +1136,53 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
                   : plan_and_launch<LFM_COMPLEX, 2, true>(P, forced, stream);
   }
   return plan_and_launch<LFM_COLOR, 2, false>(P, forced, stream);
+}
+
+
+// ---- batch launcher -------------------------------------------------------------
+namespace {
+std::mutex g_batch_mu;
+int g_batch_granted[3] = {0, 0, 0};
+
+template <typename K>
+cudaError_t grant_smem(K kernel, int smem, int* granted) {
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  if (smem <= *granted) return cudaSuccess;
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if (smem + (int)fa.sharedSizeBytes > optin) return cudaErrorNotSupported;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess) *granted = smem;
+  return e;
+}
+}  // namespace
+
+cudaError_t batch_kernel_regs(int level, int* regs) {
+  cudaFuncAttributes fa{};
+  cudaError_t e = (level == LFM_REAL) ? cudaFuncGetAttributes(&fa, tma_batch_kernel<LFM_REAL, 4>)
+                                      : cudaFuncGetAttributes(&fa, tma_batch_kernel<LFM_COMPLEX, 2>);
+  *regs = fa.numRegs;
+  return e;
+}
+
+cudaError_t launch_batch_step(int level, const BatchParams& B, int threads, int smem, int grid,
+                              cudaStream_t stream) {
+  if (B.nitems == 0) return cudaSuccess;
+  cudaError_t e;
+  if (level == LFM_REAL) {
+    e = grant_smem(tma_batch_kernel<LFM_REAL, 4>, smem, &g_batch_granted[0]);
+    if (e != cudaSuccess) return e;
+    tma_batch_kernel<LFM_REAL, 4><<<grid, threads, smem, stream>>>(B);
+  } else {
+    e = grant_smem(tma_batch_kernel<LFM_COMPLEX, 2>, smem, &g_batch_granted[1]);
+    if (e != cudaSuccess) return e;
+    tma_batch_kernel<LFM_COMPLEX, 2><<<grid, threads, smem, stream>>>(B);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace lfm

@@ -30,6 +30,23 @@ class MaskLut(ctypes.Structure):
                 ("count", c_int32)]
 
 
+class LatticeDesc(ctypes.Structure):
+    """lfm_lattice_desc: one lattice of a batch (slot pointers, mask, constants)."""
+
+    _fields_ = [("N", c_int32), ("level", c_int32), ("psi_r", c_void_p * 2),
+                ("psi_i", c_void_p * 2), ("chi", c_void_p * 2), ("mask_table", c_void_p),
+                ("lut", MaskLut), ("dt2", c_double), ("kappa", c_double),
+                ("lambda_self", c_double), ("chi0", c_double), ("e0_sq", c_double),
+                ("epsilon_w", c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    """lfm_batch_tuning: CTA size cap, stages, cells per work item, CTAs per SM (0 = default)."""
+
+    _fields_ = [("threads", c_int32), ("stages", c_int32), ("item_cells", c_int32),
+                ("ctas_per_sm", c_int32)]
+
+
 class LfmError(RuntimeError):
     """A liblfm_b200 entry point returned a non-zero status."""
 
@@ -62,6 +79,12 @@ _SIGNATURES = {
     "lfm_device_status": [POINTER(c_int), c_int],
     "lfm_metrics_f64": [_P, c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
     "lfm_metrics_f64_noalloc": [c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
+    "lfm_batch_create": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), POINTER(c_void_p)],
+    "lfm_batch_step": [_P, c_int, c_int, _P],
+    "lfm_batch_info": [_P, c_int] + [POINTER(c_int)] * 4,
+    "lfm_batch_destroy": [_P],
+    "lfm_batch_plan": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), c_int, POINTER(c_int32),
+                       c_int, POINTER(c_int), POINTER(c_int32)],
     "lfm_tune_set": [c_int] * 6,
     "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 6,
 }

@@ -90,3 +90,36 @@ def color_packets(N: int = 256, seed_phase: int = 3, seed_chi: int = 4):
     rng_c = np.random.default_rng(seed_chi)
     chi = (19.0 + rng_c.uniform(-1e-3, 1e-3, size=(N, N, N))).astype(np.float32)
     return pr.astype(np.float32), pi.astype(np.float32), chi
+
+
+def sweep_lattices(count: int = 256, seed: int = 5, sizes=(32, 48, 64, 80, 96)):
+    """Batched-sweep workload: `count` independent lattices of uneven sizes.
+
+    One generator (seed) draws, per lattice: N uniformly from `sizes`, the
+    level by a fair coin (REAL or COMPLEX), kappa = U[0.5, 2]/63, and one
+    packet at the centre with amplitude U[1, 8] and sigma U[2, 4] (COMPLEX
+    lattices give it a phase U[0, 2pi)).  chi starts at chi0.  Returns a list
+    of (config, psi_r, psi_i or None), float32 (N, N, N) fields.
+    """
+    from .config import gravity_em, gravity_only
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        N = int(rng.choice(sizes))
+        complex_level = bool(rng.integers(0, 2))
+        kappa = float(rng.uniform(0.5, 2.0)) / 63.0
+        amp = float(rng.uniform(1.0, 8.0))
+        sigma = float(rng.uniform(2.0, 4.0))
+        theta = float(rng.uniform(0.0, 2.0 * np.pi)) if complex_level else 0.0
+        cfg = (gravity_em if complex_level else gravity_only)(N, kappa=kappa)
+        c = N / 2.0
+        pr = np.zeros((N, N, N), dtype=np.float64)
+        add_gaussian(pr, (c, c, c), amp, sigma, math.cos(theta))
+        pi = None
+        if complex_level:
+            pi = np.zeros((N, N, N), dtype=np.float64)
+            add_gaussian(pi, (c, c, c), amp, sigma, math.sin(theta))
+            pi = pi.astype(np.float32)
+        out.append((cfg, pr.astype(np.float32), pi))
+    return out
