@@ -242,7 +242,7 @@ def run_reference(args):
 
 def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
     """Batched sweep: `batch_lattices` lattices (N in {32..96}, REAL/COMPLEX mixed,
-    one packet each) in one persistent launch per level and step, the whole
+    one packet each) in one persistent launch per step, the whole
     step loop replayed as one CUDA graph, against the plain loop of
     single-lattice Evolvers over the same lattices on the same GPU."""
     import torch
@@ -276,7 +276,10 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
         barrier()
         return max_over_ranks(a.elapsed_time(b))
 
-    B = BatchedLattices(cfgs, backend=be)
+    os.environ.setdefault("LFM_B200_TUNE_CACHE", str(Path(tempfile.gettempdir()) /
+                                                     "lfm_b200_bench_tune.json"))
+    B = BatchedLattices(cfgs, backend=be, tuning="auto")
+    tune = B.tune_report
     B.graph_block = steps
     for i, (c, pr, pi) in enumerate(L):
         load(B, i, pr, pi)
@@ -317,7 +320,13 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
             "speedup_vs_plain_loop": ms_p / ms_b,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "bytes_per_cell": "24 REAL / 36 COMPLEX"},
-            "launch": info, "gpu_launches": 2 * steps}
+            "launch": info, "gpu_launches": steps,
+            "autotune": {"best": tune["best"], "ms_per_step": tune["ms_per_step"],
+                         "default_ms_per_step": next(
+                             (t["ms_per_step"] for t in tune.get("trials", [])
+                              if t["tuning"] == dict(threads=256, stages=3, item_cells=65536)),
+                             None),
+                         "trials": len(tune.get("trials", []))}}
 
 
 def run_b200(args):

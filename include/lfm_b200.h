@@ -190,14 +190,17 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
 
 /* ------------------------------------------------------------------------
  * Batches of independent lattices (the runs lfm/sweep.py:14-157 makes one
- * Simulation at a time), stepped together: one launch per field level and
- * step, persistent CTAs walking a static work list of (lattice, row tile,
- * plane chunk) items sorted by cost, each item marched like the fused
- * single-lattice kernel.  REAL and COMPLEX lattices, N a multiple of 4, any
- * mix of sizes and parameters.  Each lattice keeps two slots per field in
- * the resident layout of lfm_leapfrog_*_f32: at parity p, slot p holds the
- * current fields and slot 1-p the previous ones, which the step overwrites
- * with the new fields.  damp_prev as in lfm_leapfrog_*_f32.
+ * Simulation at a time), stepped together: one launch per step, persistent
+ * CTAs taking (lattice, row tile, plane chunk) items from a work list sorted
+ * by cost (REAL and COMPLEX items on two groups of CTAs sized by the bytes
+ * each level moves), each item marched like the fused single-lattice kernel.  REAL and
+ * COMPLEX lattices, N a multiple of 4, any mix of sizes and parameters.  Each
+ * lattice keeps two slots per field in the resident layout of
+ * lfm_leapfrog_*_f32: at parity p, slot p holds the current fields and slot
+ * 1-p the previous ones, which the step overwrites with the new fields.
+ * damp_prev as in lfm_leapfrog_*_f32.  Results are bit-identical to stepping
+ * each lattice alone.  The batch owns two device counters, so launches of one
+ * batch must be ordered (one stream).
  * ------------------------------------------------------------------------ */
 typedef struct lfm_lattice_desc {
   int32_t N;
@@ -223,17 +226,19 @@ typedef struct lfm_batch lfm_batch;
  * the batch).  tuning may be NULL.  The buffers stay owned by the caller. */
 int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
                      const lfm_batch_tuning* tuning, lfm_batch** out);
-/* One step of every lattice: at most two launches (REAL, then COMPLEX). */
+/* One step of every lattice (one kernel launch). */
 int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream);
-/* Launch shape of one level's kernel (items = 0 when the batch has no lattice of it). */
-int lfm_batch_info(const lfm_batch* batch, int level, int* items, int* threads, int* grid,
-                   int* smem);
+/* Launch shape: work items, CTA size, persistent CTAs, dynamic shared memory,
+ * and how many of the CTAs run the REAL items (the rest run COMPLEX). */
+int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem,
+                   int* real_ctas);
 int lfm_batch_destroy(lfm_batch* batch);
 /* The plan lfm_batch_create would make, on the host only (no device needed;
  * 128 registers per thread and `sms` SMs assumed, 148 when sms <= 0).
- * items_out: 6 int32 per item (level, lattice, j0, j1, i0, i1), REAL items
- * first, each level in launch order; launch_out: (threads, smem, grid) per
- * level.  Either may be NULL; nitems_out gets the item count. */
+ * items_out: 6 int32 per item (level, lattice, j0, j1, i0, i1) in the order
+ * CTAs take them (REAL first); launch_out: (threads, smem, grid, real_ctas).
+ * Either may be NULL;
+ * nitems_out gets the item count. */
 int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_tuning* tuning,
                    int sms, int32_t* items_out, int max_items, int* nitems_out,
                    int32_t* launch_out);

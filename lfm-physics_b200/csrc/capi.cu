@@ -728,14 +728,13 @@ int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float
 // ---------------------------------------------------------------------------
 namespace {
 
-// Host-side plan of a batch: tile shape per lattice, one work list and one
-// launch shape per level.  Pure host arithmetic (lfm_batch_plan exposes it
-// without a device).
+// Host-side plan of a batch: tile shape per lattice, one work list (REAL
+// and COMPLEX items together) and the launch shape.  Pure host arithmetic
+// (lfm_batch_plan exposes it without a device).
 struct BatchPlan {
-  struct Level {
-    std::vector<lfm::BatchItem> items;
-    int threads = 0, smem = 0, grid = 0;
-  } lv[2];  // REAL, COMPLEX
+  std::vector<lfm::BatchItem> items;  // REAL items, then COMPLEX, each largest first
+  int real_items = 0, real_ctas = 0;
+  int threads = 0, smem = 0, grid = 0;
   std::vector<int> TJ, IC, stage_floats;
 };
 
@@ -768,59 +767,81 @@ int check_lattice_shape(const lfm_lattice_desc& d, int l) {
   return LFM_OK;
 }
 
-// regs[level]: registers per thread of the batch kernel; sms: SM count.
-int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t,
-               const int regs[2], int sms, BatchPlan* plan) {
+// Bytes a cell moves per step (the sort key's weight): REAL 6 fields x 4 B,
+// COMPLEX 9.
+inline long item_cost(const lfm::BatchItem& it, int TJ, int N) {
+  return (long)TJ * N * (it.i1 - it.i0) * (it.level == LFM_REAL ? 24 : 36);
+}
+
+// regs: registers per thread of the batch kernel; sms: SM count.
+int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, int regs,
+               int sms, BatchPlan* plan) {
   plan->TJ.assign(count, 0);
   plan->IC.assign(count, 0);
   plan->stage_floats.assign(count, 0);
-  for (int level = 0; level < 2; ++level) {
-    BatchPlan::Level& out = plan->lv[level];
+  plan->items.clear();
+  int threads = 32, max_stage = 0;
+  for (int l = 0; l < count; ++l) {
+    const int level = L[l].level;
     const int V = (level == LFM_REAL) ? 4 : 2;
     const int ns = (level == LFM_REAL) ? 2 : 3;
-    int threads = 32, max_stage = 0;
-    for (int l = 0; l < count; ++l) {
-      if (L[l].level != level) continue;
-      const int N = L[l].N;
-      const int tpr = N / V;
-      if (tpr > t.threads)
-        return fail(LFM_ERR_UNSUPPORTED, "lattice %d: a row of N=%d needs %d threads > %d", l, N,
-                    tpr, t.threads);
-      int TJ = 1;
-      for (int d = 1; d <= N; ++d)
-        if (N % d == 0 && d * tpr <= t.threads) TJ = d;
-      // chunks of about item_cells cells, the planes split as evenly as possible
-      const double cells = (double)TJ * N * N;
-      const int chunks = std::max(1, std::min(N / 2, (int)(cells / t.item_cells + 0.5)));
-      const int IC = (N + chunks - 1) / chunks;
-      plan->TJ[l] = TJ;
-      plan->IC[l] = IC;
-      // ns halo-extended fields + ns point fields (the previous-step values)
-      plan->stage_floats[l] = N * (ns * (TJ + 2) + ns * TJ);
-      max_stage = std::max(max_stage, plan->stage_floats[l]);
-      threads = std::max(threads, ((TJ * tpr + 31) / 32) * 32);
-      for (int j0 = 0; j0 < N; j0 += TJ)
-        for (int i0 = 0; i0 < N; i0 += IC) out.items.push_back({l, j0, i0, std::min(N, i0 + IC)});
-    }
-    if (out.items.empty()) continue;
-    // largest items first: the static stride then spreads the cost evenly
-    std::stable_sort(out.items.begin(), out.items.end(),
-                     [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
-                       const long ca = (long)plan->TJ[a.lattice] * L[a.lattice].N * (a.i1 - a.i0);
-                       const long cb = (long)plan->TJ[b.lattice] * L[b.lattice].N * (b.i1 - b.i0);
-                       return ca > cb;
-                     });
-    out.threads = threads;
-    out.smem = t.stages * max_stage * (int)sizeof(float);
-    if (out.smem > kBatchSmemLimit)
-      return fail(LFM_ERR_UNSUPPORTED, "batch needs %d B of shared memory per CTA (limit %d)",
-                  out.smem, kBatchSmemLimit);
-    int per_sm = std::min({(228 * 1024) / (out.smem + 1024), 2048 / threads,
-                           65536 / std::max(1, regs[level] * threads)});
-    per_sm = std::max(1, per_sm);
-    if (t.ctas_per_sm > 0) per_sm = std::min(per_sm, t.ctas_per_sm);
-    out.grid = std::min((int)out.items.size(), sms * per_sm);
+    const int N = L[l].N;
+    const int tpr = N / V;
+    if (tpr > t.threads)
+      return fail(LFM_ERR_UNSUPPORTED, "lattice %d: a row of N=%d needs %d threads > %d", l, N,
+                  tpr, t.threads);
+    int TJ = 1;
+    for (int d = 1; d <= N; ++d)
+      if (N % d == 0 && d * tpr <= t.threads) TJ = d;
+    // chunks of about item_cells cells, the planes split as evenly as possible
+    const double cells = (double)TJ * N * N;
+    const int chunks = std::max(1, std::min(N / 2, (int)(cells / t.item_cells + 0.5)));
+    const int IC = (N + chunks - 1) / chunks;
+    plan->TJ[l] = TJ;
+    plan->IC[l] = IC;
+    // ns halo-extended fields + ns point fields (the previous-step values)
+    plan->stage_floats[l] = N * (ns * (TJ + 2) + ns * TJ);
+    max_stage = std::max(max_stage, plan->stage_floats[l]);
+    threads = std::max(threads, ((TJ * tpr + 31) / 32) * 32);
+    for (int j0 = 0; j0 < N; j0 += TJ)
+      for (int i0 = 0; i0 < N; i0 += IC)
+        plan->items.push_back({l, level, j0, i0, std::min(N, i0 + IC)});
   }
+  // REAL before COMPLEX, largest first within a level: each free CTA of a
+  // level's group takes the next item (longest-processing-time order)
+  std::stable_sort(plan->items.begin(), plan->items.end(),
+                   [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
+                     if (a.level != b.level) return a.level < b.level;
+                     return item_cost(a, plan->TJ[a.lattice], L[a.lattice].N) >
+                            item_cost(b, plan->TJ[b.lattice], L[b.lattice].N);
+                   });
+  double bytes[2] = {0.0, 0.0};
+  int count_lv[2] = {0, 0};
+  for (const lfm::BatchItem& it : plan->items) {
+    bytes[it.level] += (double)item_cost(it, plan->TJ[it.lattice], L[it.lattice].N);
+    ++count_lv[it.level];
+  }
+  plan->real_items = count_lv[0];
+  plan->threads = threads;
+  plan->smem = t.stages * max_stage * (int)sizeof(float);
+  if (plan->smem > kBatchSmemLimit)
+    return fail(LFM_ERR_UNSUPPORTED, "batch needs %d B of shared memory per CTA (limit %d)",
+                plan->smem, kBatchSmemLimit);
+  int per_sm = std::min({(228 * 1024) / (plan->smem + 1024), 2048 / threads,
+                         65536 / std::max(1, regs * threads)});
+  per_sm = std::max(1, per_sm);
+  if (t.ctas_per_sm > 0) per_sm = std::min(per_sm, t.ctas_per_sm);
+  // resident CTAs split between the levels in proportion to the bytes each moves
+  const int G = sms * per_sm;
+  int g_real = 0;
+  if (count_lv[0] && count_lv[1])
+    g_real = std::max(1, std::min(G - 1, (int)std::lround(G * bytes[0] / (bytes[0] + bytes[1]))));
+  else if (count_lv[0])
+    g_real = G;
+  g_real = std::min(g_real, count_lv[0]);
+  const int g_cx = std::min(G - g_real, count_lv[1]);
+  plan->real_ctas = g_real;
+  plan->grid = g_real + g_cx;
   return LFM_OK;
 }
 
@@ -830,10 +851,9 @@ struct lfm_batch {
   int device = 0;
   int stages = 3;
   lfm::BatchLattice* d_lat = nullptr;
-  struct Level {
-    lfm::BatchItem* d_items = nullptr;
-    int nitems = 0, threads = 0, smem = 0, grid = 0;
-  } lv[2];
+  lfm::BatchItem* d_items = nullptr;
+  int* d_counters = nullptr;  // next REAL item, next COMPLEX item, retired CTAs
+  int nitems = 0, real_items = 0, real_ctas = 0, threads = 0, smem = 0, grid = 0;
 };
 
 extern "C" {
@@ -849,32 +869,29 @@ int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_
     rc = check_lattice_shape(lattices[l], l);
     if (rc) return rc;
   }
-  const int regs[2] = {128, 128};
   BatchPlan plan;
-  rc = plan_batch(lattices, count, t, regs, sms > 0 ? sms : 148, &plan);
+  rc = plan_batch(lattices, count, t, 128, sms > 0 ? sms : 148, &plan);
   if (rc) return rc;
-  const int total = (int)(plan.lv[0].items.size() + plan.lv[1].items.size());
+  const int total = (int)plan.items.size();
   if (nitems_out) *nitems_out = total;
   if (items_out) {
     if (max_items < total) return fail(LFM_ERR_CAPACITY, "%d items > capacity %d", total, max_items);
-    int k = 0;
-    for (int lv = 0; lv < 2; ++lv)
-      for (const lfm::BatchItem& it : plan.lv[lv].items) {
-        items_out[6 * k + 0] = lv;
-        items_out[6 * k + 1] = it.lattice;
-        items_out[6 * k + 2] = it.j0;
-        items_out[6 * k + 3] = it.j0 + plan.TJ[it.lattice];
-        items_out[6 * k + 4] = it.i0;
-        items_out[6 * k + 5] = it.i1;
-        ++k;
-      }
-  }
-  if (launch_out)
-    for (int lv = 0; lv < 2; ++lv) {
-      launch_out[3 * lv + 0] = plan.lv[lv].threads;
-      launch_out[3 * lv + 1] = plan.lv[lv].smem;
-      launch_out[3 * lv + 2] = plan.lv[lv].grid;
+    for (int k = 0; k < total; ++k) {
+      const lfm::BatchItem& it = plan.items[k];
+      items_out[6 * k + 0] = it.level;
+      items_out[6 * k + 1] = it.lattice;
+      items_out[6 * k + 2] = it.j0;
+      items_out[6 * k + 3] = it.j0 + plan.TJ[it.lattice];
+      items_out[6 * k + 4] = it.i0;
+      items_out[6 * k + 5] = it.i1;
     }
+  }
+  if (launch_out) {
+    launch_out[0] = plan.threads;
+    launch_out[1] = plan.smem;
+    launch_out[2] = plan.grid;
+    launch_out[3] = plan.real_ctas;
+  }
   return LFM_OK;
 }
 
@@ -913,11 +930,9 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
                                 0, 0, 0);
     b.lut = device_lut(d.mask_table, &d.lut);
   }
-  int regs[2] = {128, 128};
-  for (int lv = 0; lv < 2; ++lv) {
-    cudaError_t e = lfm::batch_kernel_regs(lv, &regs[lv]);
-    if (e != cudaSuccess) return cuda_fail(e, "batch kernel attributes");
-  }
+  int regs = 128;
+  cudaError_t e = lfm::batch_kernel_regs(&regs);
+  if (e != cudaSuccess) return cuda_fail(e, "batch kernel attributes");
   int device = 0, sms = 148;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -932,22 +947,23 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
   lfm_batch* B = new lfm_batch;
   B->device = device;
   B->stages = t.stages;
-  cudaError_t e = cudaMalloc(&B->d_lat, sizeof(lfm::BatchLattice) * count);
+  B->nitems = (int)plan.items.size();
+  B->real_items = plan.real_items;
+  B->real_ctas = plan.real_ctas;
+  B->threads = plan.threads;
+  B->smem = plan.smem;
+  B->grid = plan.grid;
+  e = cudaMalloc(&B->d_lat, sizeof(lfm::BatchLattice) * count);
   if (e == cudaSuccess)
     e = cudaMemcpy(B->d_lat, dev.data(), sizeof(lfm::BatchLattice) * count,
                    cudaMemcpyHostToDevice);
-  for (int lv = 0; lv < 2 && e == cudaSuccess; ++lv) {
-    const std::vector<lfm::BatchItem>& items = plan.lv[lv].items;
-    B->lv[lv].nitems = (int)items.size();
-    B->lv[lv].threads = plan.lv[lv].threads;
-    B->lv[lv].smem = plan.lv[lv].smem;
-    B->lv[lv].grid = plan.lv[lv].grid;
-    if (items.empty()) continue;
-    e = cudaMalloc(&B->lv[lv].d_items, sizeof(lfm::BatchItem) * items.size());
-    if (e == cudaSuccess)
-      e = cudaMemcpy(B->lv[lv].d_items, items.data(), sizeof(lfm::BatchItem) * items.size(),
-                     cudaMemcpyHostToDevice);
-  }
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_items, sizeof(lfm::BatchItem) * plan.items.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(B->d_items, plan.items.data(), sizeof(lfm::BatchItem) * plan.items.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_counters, 3 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(B->d_counters, 0, 3 * sizeof(int));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     lfm_batch_destroy(B);
     return cuda_fail(e, "batch descriptors");
@@ -962,33 +978,32 @@ int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
   int* status = nullptr;
   int rc = status_word(&status);
   if (rc) return rc;
-  for (int lv = 0; lv < 2; ++lv) {
-    const lfm_batch::Level& L = batch->lv[lv];
-    if (!L.nitems) continue;
-    lfm::BatchParams P{};
-    P.lattices = batch->d_lat;
-    P.items = L.d_items;
-    P.nitems = L.nitems;
-    P.parity = parity;
-    P.damp_prev = damp_prev ? 1 : 0;
-    P.stages = batch->stages;
-    P.status = status;
-    cudaError_t e = lfm::launch_batch_step(lv, P, L.threads, L.smem, L.grid,
-                                           static_cast<cudaStream_t>(stream));
-    if (e != cudaSuccess) return cuda_fail(e, "batch step launch");
-  }
+  lfm::BatchParams P{};
+  P.lattices = batch->d_lat;
+  P.items = batch->d_items;
+  P.nitems = batch->nitems;
+  P.real_items = batch->real_items;
+  P.real_ctas = batch->real_ctas;
+  P.parity = parity;
+  P.damp_prev = damp_prev ? 1 : 0;
+  P.stages = batch->stages;
+  P.status = status;
+  P.next_item = batch->d_counters;
+  P.retired = batch->d_counters + 2;
+  cudaError_t e = lfm::launch_batch_step(P, batch->threads, batch->smem, batch->grid,
+                                         static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "batch step launch");
   return LFM_OK;
 }
 
-int lfm_batch_info(const lfm_batch* batch, int level, int* items, int* threads, int* grid,
-                   int* smem) {
+int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem,
+                   int* real_ctas) {
   if (!batch) return fail(LFM_ERR_INVALID_ARG, "null batch");
-  if (level != LFM_REAL && level != LFM_COMPLEX) return fail(LFM_ERR_INVALID_ARG, "level %d", level);
-  const lfm_batch::Level& L = batch->lv[level];
-  if (items) *items = L.nitems;
-  if (threads) *threads = L.threads;
-  if (grid) *grid = L.grid;
-  if (smem) *smem = L.smem;
+  if (real_ctas) *real_ctas = batch->real_ctas;
+  if (items) *items = batch->nitems;
+  if (threads) *threads = batch->threads;
+  if (grid) *grid = batch->grid;
+  if (smem) *smem = batch->smem;
   return LFM_OK;
 }
 
@@ -998,8 +1013,8 @@ int lfm_batch_destroy(lfm_batch* batch) {
   cudaGetDevice(&prev);
   cudaSetDevice(batch->device);
   if (batch->d_lat) cudaFree(batch->d_lat);
-  for (auto& L : batch->lv)
-    if (L.d_items) cudaFree(L.d_items);
+  if (batch->d_items) cudaFree(batch->d_items);
+  if (batch->d_counters) cudaFree(batch->d_counters);
   cudaSetDevice(prev);
   delete batch;
   return LFM_OK;

@@ -25,24 +25,29 @@ struct BatchLattice {
 
 struct BatchItem {
   int lattice;
+  int level;  // LFM_REAL or LFM_COMPLEX, copied from the lattice
   int j0, i0, i1;
 };
 
 struct BatchParams {
   const BatchLattice* lattices;
-  const BatchItem* items;
+  const BatchItem* items;  // REAL items first, then COMPLEX, each sorted by cost
   int nitems;
+  int real_items;  // items[0, real_items) are REAL
+  int real_ctas;   // CTAs [0, real_ctas) run the REAL items
   int parity;     // slot holding the current fields
   int damp_prev;  // previous-field slots hold undamped values
   int stages;
   int* status;
+  int* next_item;  // work-list counters (REAL, COMPLEX), 0 between launches
+  int* retired;    // CTAs that took their last item, 0 between launches
 };
 
-// Launches one step of every lattice of one level (REAL or COMPLEX).
-cudaError_t launch_batch_step(int level, const BatchParams& B, int threads, int smem, int grid,
+// Launches one step of every lattice of the batch.
+cudaError_t launch_batch_step(const BatchParams& B, int threads, int smem, int grid,
                               cudaStream_t stream);
 
-// Registers per thread of the batch kernel of a level (for the planner).
-cudaError_t batch_kernel_regs(int level, int* regs);
+// Registers per thread of the batch kernel (for the planner).
+cudaError_t batch_kernel_regs(int* regs);
 
 }  // namespace lfm

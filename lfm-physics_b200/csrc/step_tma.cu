@@ -574,13 +574,15 @@ struct QShared {
 // the centre plane's stage when it is done with it, and the last warp to do
 // so refills the stage with the plane S further on.  Returns false when the
 // CTA must stop (a bounded wait gave up).
-template <int LEVEL, int V, bool COMP, int PA, int PB, int PC>
+template <int LEVEL, int V, bool COMP, bool PARTIAL, int PA, int PB, int PC>
 __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
                                         const QLane& L, int c, int i0, int i1, int j0,
                                         int nplanes, int nwarps, int& s_cur, int& s_nxt,
                                         uint32_t& ph_nxt, int32_t qj, const int32_t (&qk)[V],
-                                        bool active) {
+                                        bool lane_active) {
+  // PARTIAL: the CTA may be wider than the tile (batch kernel)
+  const bool active = !PARTIAL || lane_active;
   constexpr int NS = QFields<LEVEL>::ns;
   const StepArgs& a = P.a;
   const int N = P.N, TJ = P.TJ;
@@ -724,7 +726,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
 // The march of one tile: rows j0 .. j0+rows-1 (all k), planes [i0, i1).
 // Initialises the stage barriers and the bookkeeping itself, so a CTA may
 // run several marches one after another (the batch kernel).
-template <int LEVEL, int V, bool COMP>
+template <int LEVEL, int V, bool COMP, bool PARTIAL>
 __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, int j0, int i0, int i1, int rows) {
   constexpr int NS = QFields<LEVEL>::ns;
@@ -734,7 +736,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   const int tid = threadIdx.x;
   const int nwarps = blockDim.x >> 5;
   const int tpr = N / V;
-  const bool active = tid < rows * tpr;
+  const bool active = !PARTIAL || tid < rows * tpr;
   const int r = active ? tid / tpr : 0;
   const int k0 = active ? (tid % tpr) * V : 0;
   const int km1 = (k0 == 0) ? N - 1 : k0 - 1;
@@ -799,15 +801,15 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     uint32_t ph_nxt = (uint32_t)((2 / S) & 1);
     int c = 0;
     while (true) {
-      if (c >= n || !q_plane<LEVEL, V, COMP, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+      if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
                                                       nplanes, nwarps, s_cur, s_nxt, ph_nxt, qj,
                                                       qk, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
                                                         nplanes, nwarps, s_cur, s_nxt, ph_nxt,
                                                         qj, qk, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
+      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
                                                         nplanes, nwarps, s_cur, s_nxt, ph_nxt,
                                                         qj, qk, active))
         break;
@@ -830,72 +832,106 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
   __shared__ QShared sh;
   const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
   const int i0 = ch * P.IC;
-  q_march<LEVEL, V, COMP>(P, smem, bars, sh, jt * P.TJ, i0, min(i0 + P.IC, P.N), P.TJ);
+  q_march<LEVEL, V, COMP, false>(P, smem, bars, sh, jt * P.TJ, i0, min(i0 + P.IC, P.N), P.TJ);
 }
 
-// ---- batch kernel: many lattices, one launch per level and step ---------------
+// ---- batch kernel: many lattices, one launch per step -------------------------
 //
-// Persistent CTAs walk a static work list of (lattice, row tile, plane chunk)
-// items, sorted by cost, and run the same barrier-free march on each.  The
-// per-item parameters (slot pointers for this step's parity, constants, mask
-// table, tile shape) are built in shared memory from the lattice descriptor.
+// Persistent CTAs take (lattice, row tile, plane chunk) items from a work list
+// sorted by cost, through a device counter (largest first, next free CTA takes
+// the next item), and run the same barrier-free march on each.  REAL and
+// COMPLEX items share the launch.  The per-item parameters (slot pointers for
+// this step's parity, constants, mask table, tile shape) are built in shared
+// memory from the lattice descriptor.  The last CTA to retire rewinds the
+// counters for the next launch on the stream.
+template <int LEVEL>
+__device__ __forceinline__ void batch_params(TmaParams& P, const BatchLattice& L,
+                                             const BatchParams& B) {
+  const int cur = B.parity, nxt = 1 - B.parity;
+  StepArgs a{};
+  a.level = LEVEL;
+  a.N = L.N;
+  a.c = L.c;
+  a.pr = L.pr[cur];
+  a.pr_prev = L.pr[nxt];
+  a.pr_out = L.pr[nxt];
+  a.chi = L.chi[cur];
+  a.chi_prev = L.chi[nxt];
+  a.chi_out = L.chi[nxt];
+  if (LEVEL == LFM_COMPLEX) {
+    a.pi = L.pi[cur];
+    a.pi_prev = L.pi[nxt];
+    a.pi_out = L.pi[nxt];
+  }
+  a.lut = L.lut;
+  a.damp_prev = B.damp_prev;
+  a.status = B.status;
+  P.a = a;
+  if (LEVEL == LFM_REAL) {
+    P.ns = 2;
+    P.sf[0] = a.pr; P.sf[1] = a.chi;
+    P.np = 2;
+    P.pf[0] = a.pr_prev; P.pf[1] = a.chi_prev;
+  } else {
+    P.ns = 3;
+    P.sf[0] = a.pr; P.sf[1] = a.pi; P.sf[2] = a.chi;
+    P.np = 3;
+    P.pf[0] = a.pr_prev; P.pf[1] = a.pi_prev; P.pf[2] = a.chi_prev;
+  }
+  P.pf_mask = -1;
+  P.pf_sa = -1;
+  P.N = L.N;
+  P.TJ = L.TJ;
+  P.IC = L.IC;
+  P.S = B.stages;
+  P.JT = L.N / L.TJ;
+  P.stage_floats = L.stage_floats;
+}
+
+// The item loop of one level: CTAs take items through that level's counter.
 template <int LEVEL, int V>
+__device__ __forceinline__ void batch_level(const BatchParams& B, const BatchItem* items,
+                                            int nitems, int* next_item, float* smem,
+                                            uint64_t* bars, QShared& sh, TmaParams& P,
+                                            int& s_item) {
+  while (true) {
+    __syncthreads();  // every warp is done with the previous item
+    if (threadIdx.x == 0) s_item = atomicAdd(next_item, 1);
+    __syncthreads();
+    const int w = s_item;
+    if (w >= nitems) break;
+    const BatchItem it = items[w];
+    if (threadIdx.x == 0) batch_params<LEVEL>(P, B.lattices[it.lattice], B);
+    __syncthreads();  // P is visible to every thread
+    q_march<LEVEL, V, false, true>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
+    __syncthreads();  // every wait of the march is over
+    if (sh.abort_flag) break;  // same value in every thread
+    if (threadIdx.x == 0)
+      for (int s = 0; s < B.stages; ++s) mbar_inval(&bars[s]);  // the next march re-initialises
+  }
+}
+
+// CTAs [0, real_ctas) run the REAL items, the others the COMPLEX ones (the
+// split follows the bytes each level moves).
 __global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ BatchParams B) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
   __shared__ QShared sh;
   __shared__ TmaParams P;
-  for (int w = blockIdx.x; w < B.nitems; w += gridDim.x) {
-    const BatchItem it = B.items[w];
-    __syncthreads();  // every warp is done with the previous item's parameters
-    if (threadIdx.x == 0) {
-      const BatchLattice& L = B.lattices[it.lattice];
-      const int cur = B.parity, nxt = 1 - B.parity;
-      StepArgs a{};
-      a.level = LEVEL;
-      a.N = L.N;
-      a.c = L.c;
-      a.pr = L.pr[cur];
-      a.pr_prev = L.pr[nxt];
-      a.pr_out = L.pr[nxt];
-      a.chi = L.chi[cur];
-      a.chi_prev = L.chi[nxt];
-      a.chi_out = L.chi[nxt];
-      if (LEVEL == LFM_COMPLEX) {
-        a.pi = L.pi[cur];
-        a.pi_prev = L.pi[nxt];
-        a.pi_out = L.pi[nxt];
-      }
-      a.lut = L.lut;
-      a.damp_prev = B.damp_prev;
-      a.status = B.status;
-      P.a = a;
-      if (LEVEL == LFM_REAL) {
-        P.ns = 2;
-        P.sf[0] = a.pr; P.sf[1] = a.chi;
-        P.np = 2;
-        P.pf[0] = a.pr_prev; P.pf[1] = a.chi_prev;
-      } else {
-        P.ns = 3;
-        P.sf[0] = a.pr; P.sf[1] = a.pi; P.sf[2] = a.chi;
-        P.np = 3;
-        P.pf[0] = a.pr_prev; P.pf[1] = a.pi_prev; P.pf[2] = a.chi_prev;
-      }
-      P.pf_mask = -1;
-      P.pf_sa = -1;
-      P.N = L.N;
-      P.TJ = L.TJ;
-      P.IC = L.IC;
-      P.S = B.stages;
-      P.JT = L.N / L.TJ;
-      P.stage_floats = L.stage_floats;
+  __shared__ int s_item;
+  if ((int)blockIdx.x < B.real_ctas)
+    batch_level<LFM_REAL, 4>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P, s_item);
+  else
+    batch_level<LFM_COMPLEX, 2>(B, B.items + B.real_items, B.nitems - B.real_items,
+                                B.next_item + 1, smem, bars, sh, P, s_item);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(B.retired, 1) == (int)gridDim.x - 1) {
+      // every CTA has taken its last item: rewind for the next launch
+      atomicExch(B.next_item, 0);
+      atomicExch(B.next_item + 1, 0);
+      atomicExch(B.retired, 0);
     }
-    __syncthreads();  // P is visible to every thread
-    q_march<LEVEL, V, false>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
-    __syncthreads();  // every wait of the march is over
-    if (sh.abort_flag) break;  // same value in every thread
-    if (threadIdx.x == 0)
-      for (int s = 0; s < P.S; ++s) mbar_inval(&bars[s]);  // re-initialised by the next march
   }
 }
 
@@ -1142,7 +1178,7 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
 // ---- batch launcher -------------------------------------------------------------
 namespace {
 std::mutex g_batch_mu;
-int g_batch_granted[3] = {0, 0, 0};
+int g_batch_granted = 0;  // dynamic shared memory granted to the batch kernel
 
 template <typename K>
 cudaError_t grant_smem(K kernel, int smem, int* granted) {
@@ -1161,27 +1197,19 @@ cudaError_t grant_smem(K kernel, int smem, int* granted) {
 }
 }  // namespace
 
-cudaError_t batch_kernel_regs(int level, int* regs) {
+cudaError_t batch_kernel_regs(int* regs) {
   cudaFuncAttributes fa{};
-  cudaError_t e = (level == LFM_REAL) ? cudaFuncGetAttributes(&fa, tma_batch_kernel<LFM_REAL, 4>)
-                                      : cudaFuncGetAttributes(&fa, tma_batch_kernel<LFM_COMPLEX, 2>);
-  *regs = fa.numRegs;
+  cudaError_t e = cudaFuncGetAttributes(&fa, tma_batch_kernel);
+  if (e == cudaSuccess) *regs = fa.numRegs;
   return e;
 }
 
-cudaError_t launch_batch_step(int level, const BatchParams& B, int threads, int smem, int grid,
+cudaError_t launch_batch_step(const BatchParams& B, int threads, int smem, int grid,
                               cudaStream_t stream) {
   if (B.nitems == 0) return cudaSuccess;
-  cudaError_t e;
-  if (level == LFM_REAL) {
-    e = grant_smem(tma_batch_kernel<LFM_REAL, 4>, smem, &g_batch_granted[0]);
-    if (e != cudaSuccess) return e;
-    tma_batch_kernel<LFM_REAL, 4><<<grid, threads, smem, stream>>>(B);
-  } else {
-    e = grant_smem(tma_batch_kernel<LFM_COMPLEX, 2>, smem, &g_batch_granted[1]);
-    if (e != cudaSuccess) return e;
-    tma_batch_kernel<LFM_COMPLEX, 2><<<grid, threads, smem, stream>>>(B);
-  }
+  cudaError_t e = grant_smem(tma_batch_kernel, smem, &g_batch_granted);
+  if (e != cudaSuccess) return e;
+  tma_batch_kernel<<<grid, threads, smem, stream>>>(B);
   return cudaGetLastError();
 }
 

@@ -81,7 +81,7 @@ _SIGNATURES = {
     "lfm_metrics_f64_noalloc": [c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
     "lfm_batch_create": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), POINTER(c_void_p)],
     "lfm_batch_step": [_P, c_int, c_int, _P],
-    "lfm_batch_info": [_P, c_int] + [POINTER(c_int)] * 4,
+    "lfm_batch_info": [_P] + [POINTER(c_int)] * 5,
     "lfm_batch_destroy": [_P],
     "lfm_batch_plan": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), c_int, POINTER(c_int32),
                        c_int, POINTER(c_int), POINTER(c_int32)],

@@ -4,8 +4,8 @@ The reference runs a parameter sweep one ``Simulation`` after another
 (lfm/sweep.py:52-82: deep-copy the config, build, run, read metrics).  Small
 lattices leave most of a B200 idle that way.  ``BatchedLattices`` holds every
 lattice of a sweep resident in one device arena and advances all of them with
-one persistent kernel launch per field level and step (lfm_batch_step): the
-CTAs walk a static work list of (lattice, row tile, plane chunk) items, each
+one persistent kernel launch per step (lfm_batch_step): the CTAs take
+(lattice, row tile, plane chunk) items from a cost-sorted work list, each
 marched exactly like the fused single-lattice kernel, so every lattice's
 result is bit-for-bit the one ``Evolver`` gives for it alone.
 
@@ -31,12 +31,15 @@ _ALIGN = 64  # floats: every slot starts on a 256-byte boundary
 
 
 class BatchedLattices:
-    """REAL / COMPLEX lattices of mixed sizes, one persistent launch per level and step."""
+    """REAL / COMPLEX lattices of mixed sizes, one persistent launch per step."""
 
     graph_block = 16
     """Steps per captured CUDA graph (an even number)."""
 
-    def __init__(self, configs, backend="auto", tuning: dict | None = None) -> None:
+    def __init__(self, configs, backend="auto", tuning: dict | str | None = None) -> None:
+        """configs: SimulationConfig per lattice.  tuning: None (defaults), a dict
+        of lfm_batch_tuning fields, or "auto" (lfm_b200.autotune.tune_batch,
+        cached per device and (N, level) mix)."""
         import torch
 
         self.configs = list(configs)
@@ -99,16 +102,34 @@ class BatchedLattices:
             d.chi0 = float(c.chi0)
             d.e0_sq = float(c.e0_sq)
             d.epsilon_w = float(c.epsilon_w)
-        self._tuning = _lib.BatchTuning()
-        for k, v in (tuning or {}).items():
-            setattr(self._tuning, k, int(v))
-        h = ctypes.c_void_p()
-        _lib.call("lfm_batch_create", self._descs, len(self.configs), ctypes.byref(self._tuning),
-                  ctypes.byref(h))
-        self._handle = h
+        self._handle = None
         self._cur = 0
         self._damp = False
         self._graphs: dict = {}
+        self.tune_report = None
+        if tuning == "auto":
+            from .autotune import tune_batch
+
+            self.retune(None)
+            self.tune_report = tune_batch(self)
+        else:
+            self.retune(tuning)
+
+    def retune(self, tuning: dict | None) -> None:
+        """Re-plan the work list with another tuning (keys of lfm_batch_tuning:
+        threads, stages, item_cells, ctas_per_sm; missing or 0 = default).
+        The fields are untouched; captured graphs are dropped."""
+        t = _lib.BatchTuning()
+        for k, v in (tuning or {}).items():
+            setattr(t, k, int(v))
+        h = ctypes.c_void_p()
+        _lib.call("lfm_batch_create", self._descs, len(self.configs), ctypes.byref(t),
+                  ctypes.byref(h))
+        self._graphs = {}
+        if self._handle:
+            _lib.load().lfm_batch_destroy(self._handle)
+        self._handle = h
+        self._tuning = {f: getattr(t, f) for f, _ in t._fields_}
 
     def __len__(self) -> int:
         return len(self.configs)
@@ -127,13 +148,11 @@ class BatchedLattices:
 
     # ---------------------------------------------------------------- plan
     def info(self) -> dict:
-        """Launch shape per level: items, threads, grid, shared memory."""
-        out = {}
-        for lv, name in ((0, "real"), (1, "complex")):
-            v = [ctypes.c_int(0) for _ in range(4)]
-            _lib.call("lfm_batch_info", self._handle, lv, *[ctypes.byref(x) for x in v])
-            out[name] = dict(zip(("items", "threads", "grid", "smem"), (x.value for x in v)))
-        return out
+        """Launch shape: work items, threads per CTA, persistent CTAs, shared memory,
+        CTAs of the REAL group."""
+        v = [ctypes.c_int(0) for _ in range(5)]
+        _lib.call("lfm_batch_info", self._handle, *[ctypes.byref(x) for x in v])
+        return dict(zip(("items", "threads", "grid", "smem", "real_ctas"), (x.value for x in v)))
 
     # ---------------------------------------------------------------- stepping
     def _step(self) -> None:
@@ -318,7 +337,7 @@ def plan(configs, tuning: dict | None = None, sms: int = 148) -> dict:
     """The work list lfm_batch_create would build for these configs (host only, no device).
 
     Returns {"items": int32 array (n, 6) of (level, lattice, j0, j1, i0, i1),
-    "launch": {"real": (threads, smem, grid), "complex": (...)}}.
+    "launch": (threads, smem, grid, real_ctas)}.
     """
     descs = (_lib.LatticeDesc * len(configs))()
     for i, c in enumerate(configs):
@@ -332,11 +351,10 @@ def plan(configs, tuning: dict | None = None, sms: int = 148) -> dict:
     _lib.check(lib.lfm_batch_plan(descs, len(configs), ctypes.byref(t), int(sms), None, 0,
                                   ctypes.byref(n), None), "lfm_batch_plan")
     items = np.zeros((max(n.value, 1), 6), dtype=np.int32)
-    launch = np.zeros(6, dtype=np.int32)
+    launch = np.zeros(4, dtype=np.int32)
     i32p = ctypes.POINTER(ctypes.c_int32)
     _lib.check(lib.lfm_batch_plan(descs, len(configs), ctypes.byref(t), int(sms),
                                   items.ctypes.data_as(i32p), items.shape[0], ctypes.byref(n),
                                   launch.ctypes.data_as(i32p)), "lfm_batch_plan")
     return {"items": items[:n.value],
-            "launch": {"real": tuple(int(x) for x in launch[0:3]),
-                       "complex": tuple(int(x) for x in launch[3:6])}}
+            "launch": tuple(int(x) for x in launch)}

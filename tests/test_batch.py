@@ -62,14 +62,16 @@ def test_plan_covers_every_cell_once(lib, tuning):
     cfgs = [c for c, _, _ in sweep_lattices(64, seed=5)] + mixed_configs([8, 12, 16, 20, 100])
     p = batch.plan(cfgs, tuning)
     check_coverage(cfgs, p["items"])
-    for name, (threads, smem, grid) in p["launch"].items():
-        assert threads % 32 == 0 and 0 < threads <= (tuning or {}).get("threads", 256)
-        assert 0 < smem <= 226 * 1024 and 0 < grid
-    # each level's list runs largest items first
+    threads, smem, grid, real_ctas = p["launch"]
+    assert threads % 32 == 0 and 0 < threads <= (tuning or {}).get("threads", 256)
+    assert 0 < smem <= 226 * 1024 and 0 < real_ctas < grid
+    # REAL items first, then COMPLEX; each level runs largest items first
+    it = p["items"]
+    assert (np.diff(it[:, 0]) >= 0).all()
     for lvl in (0, 1):
-        it = p["items"][p["items"][:, 0] == lvl]
-        N = np.array([cfgs[l].grid_size for l in it[:, 1]])
-        cost = (it[:, 3] - it[:, 2]) * N * (it[:, 5] - it[:, 4])
+        sub = it[it[:, 0] == lvl]
+        N = np.array([cfgs[l].grid_size for l in sub[:, 1]])
+        cost = (sub[:, 3] - sub[:, 2]) * N * (sub[:, 5] - sub[:, 4])
         assert (np.diff(cost) <= 0).all()
 
 
@@ -82,7 +84,12 @@ def test_plan_of_the_sweep_workload(lib):
     assert {c.grid_size for c in cfgs} == {32, 48, 64, 80, 96}
     p = batch.plan(cfgs)
     check_coverage(cfgs, p["items"])
-    assert p["launch"]["real"][2] == 296 and p["launch"]["complex"][2] == 296
+    threads, smem, grid, real_ctas = p["launch"]
+    assert grid == 296
+    # the CTA split follows the bytes: 24 B/cell REAL, 36 B/cell COMPLEX
+    br = sum(c.grid_size**3 * 24 for c in cfgs if int(c.field_level) == 0)
+    bc = sum(c.grid_size**3 * 36 for c in cfgs if int(c.field_level) == 1)
+    assert abs(real_ctas - 296 * br / (br + bc)) <= 1.0
 
 
 @pytest.mark.parametrize("bad, code", [(dict(N=10), 3), (dict(level=2), 3), (dict(N=4), 3)])
@@ -258,3 +265,54 @@ def test_sweep_workload_subset(be):
         assert bits_equal(B.get_chi(i), ev.get_chi()), i
         m = B.metrics(i)
         assert m["nonfinite_cells"] == 0
+
+
+@pytest.mark.gpu
+def test_autotune_batch_keeps_state_and_bits(be, tmp_path, monkeypatch):
+    from lfm_b200 import autotune
+
+    monkeypatch.setenv("LFM_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    cfgs = mixed_configs([16, 20, 32, 24])
+    B, evs = run_pair(be, cfgs, 5)
+    before = [B.get_psi_real(i) for i in range(len(cfgs))]
+    rep = autotune.tune_batch(B, candidates=[dict(threads=128), dict(threads=256, stages=4),
+                                             dict(item_cells=2048)], steps=3)
+    assert len(rep["trials"]) == 3 and rep["best"] in [t["tuning"] for t in rep["trials"]]
+    assert all(bits_equal(B.get_psi_real(i), b) for i, b in enumerate(before))
+    assert B.step == 5
+    B.evolve(6)
+    for ev in evs:
+        ev.evolve(6)
+    assert_same(B, evs)
+    # full search with the cache: a second call is a cache hit
+    r1 = autotune.tune_batch(B, steps=2)
+    r2 = autotune.tune_batch(B, steps=2)
+    assert r1["best"] == r2["best"] and (tmp_path / "tune.json").exists()
+
+
+@pytest.mark.gpu
+def test_autotune_lattice_pins_a_tile(be, tmp_path, monkeypatch):
+    from lfm_b200 import Evolver, _lib, autotune
+    from lfm_b200.config import gravity_only
+
+    monkeypatch.setenv("LFM_B200_TUNE_CACHE", str(tmp_path / "tune.json"))
+    cfg = gravity_only(32)
+    rng = np.random.default_rng(1)
+    pr, _, chi = seed_fields(cfg, rng)
+    ev, ref = Evolver(cfg, backend=be), Evolver(cfg, backend=be)
+    for e in (ev, ref):
+        e.set_psi_real(pr)
+        e.set_chi(chi)
+        e.evolve(3)
+    rep = autotune.tune_lattice(ev, candidates=[dict(vec=4, tj=8, stages=3, ic=0),
+                                                dict(vec=2, tj=4, stages=4, ic=16)], steps=3)
+    try:
+        assert len(rep["trials"]) == 2
+        assert ev.step == 3
+        ev.evolve(8)
+        assert _lib.tune_get(0, 32)["tj"] == rep["best"]["tj"]  # the pinned tile ran
+        ref.evolve(8)
+        assert bits_equal(ev.get_psi_real(), ref.get_psi_real())
+        assert bits_equal(ev.get_chi(), ref.get_chi())
+    finally:
+        _lib.tune_set(0, 32, 0, 0, 0, 0)
