@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-lattices", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-steps", type=int, default=500)
     return ap.parse_args()
 
 
@@ -329,6 +331,84 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
                          "trials": len(tune.get("trials", []))}}
 
 
+def run_adjoint(args, be, dev, barrier, max_over_ranks):
+    """Gradient of |chi_final - chi_target|^2 through `adjoint_steps` COMPLEX 96^3
+    steps (gravity_em: lambda = 4/31, eps_w = 0.1) with respect to the
+    amplitude, centre and phase of two packets and a per-cell chi offset; the
+    target is a forward run from perturbed packet parameters (seed 6).
+    Forward = the checkpointed forward pass, backward = recompute + adjoint."""
+    import math
+
+    import torch
+
+    from lfm_b200 import Evolver
+    from lfm_b200.adjoint import leapfrog, memory_bytes, soliton_state
+    from lfm_b200.config import gravity_em
+
+    N, steps, sigma = 96, args.adjoint_steps, 3.0
+    cfg = gravity_em(N)
+    g = torch.Generator().manual_seed(6)
+    amp = 2.0 + 2.0 * torch.rand(2, generator=g)
+    cen = torch.tensor([[N / 2 - 10.0, N / 2, N / 2], [N / 2 + 10.0, N / 2, N / 2]])
+    ph = 2.0 * math.pi * torch.rand(2, generator=g)
+    pert = (amp * (1.0 + 0.05 * torch.randn(2, generator=g)),
+            cen + 0.5 * torch.randn(2, 3, generator=g), ph + 0.1 * torch.randn(2, generator=g))
+    params = [t.to(dev) for t in (amp, cen, ph)]
+    with torch.no_grad():
+        st = soliton_state(N, *[t.to(dev) for t in pert], sigma, cfg.chi0, None, True)
+        target = leapfrog(cfg, st, steps, backend=be)[4].clone()
+    stream = torch.cuda.current_stream(dev)
+
+    def one(timed: bool):
+        p = [t.clone().requires_grad_(True) for t in params]
+        dchi = torch.zeros((N, N, N), device=dev, requires_grad=True)
+        st = soliton_state(N, *p, sigma, cfg.chi0, dchi, True)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize(dev)
+        barrier()
+        ev[0].record(stream)
+        out = leapfrog(cfg, st, steps, backend=be)
+        ev[1].record(stream)
+        loss = ((out[4] - target) ** 2).sum()
+        loss.backward()
+        ev[2].record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        fwd = max_over_ranks(ev[0].elapsed_time(ev[1]))
+        bwd = max_over_ranks(ev[1].elapsed_time(ev[2]))
+        return fwd, bwd, float(loss), [float(q.grad.abs().max()) for q in p] + [
+            float(dchi.grad.abs().max())]
+
+    one(False)
+    torch.cuda.reset_peak_memory_stats(dev)
+    base = torch.cuda.memory_allocated(dev)
+    fwd, bwd, loss, gmax = one(True)
+    peak = torch.cuda.max_memory_allocated(dev) - base
+    # the plain forward of the same steps (Evolver, two-step CUDA graphs)
+    evp = Evolver(cfg, backend=be)
+    evp.set_psi_real(st[0])
+    evp.set_psi_imag(st[2])
+    evp.evolve(5)
+    evp.warm_graphs()
+    torch.cuda.synchronize(dev)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    evp.evolve(steps)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    plain = max_over_ranks(a.elapsed_time(b))
+    mem = memory_bytes(cfg, steps)
+    return {"workload": f"COMPLEX {N}^3 gravity_em, {steps} steps, two packets + per-cell "
+                        "chi offset, loss |chi - chi_target|^2",
+            "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "backward_over_plain_forward": bwd / plain, "plain_forward_ms": plain,
+            "loss": loss, "grad_max": dict(zip(("amplitude", "centre", "phase", "dchi"), gmax)),
+            "checkpoints": mem["checkpoints"], "checkpoint_bytes": mem["checkpoint_bytes"],
+            "segment_bytes": mem["segment_bytes"], "all_states_bytes": mem["all_states_bytes"],
+            "peak_extra_bytes": peak}
+
+
 def run_b200(args):
     import numpy as np
     import torch
@@ -422,6 +502,10 @@ def run_b200(args):
                 "tile": _lib.tune_get(0, N)}
         del evc
 
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(args, be, dev, barrier, max_over_ranks)
+
     batched = None
     if not args.no_batched:
         batched = run_batched(args, be, dev, rank, barrier, max_over_ranks, peak)
@@ -486,6 +570,8 @@ def run_b200(args):
         line["compensated"] = comp
     if batched is not None:
         line["batched"] = batched
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
     if world > 1:

@@ -189,6 +189,24 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
                                   double e0_sq, double epsilon_w, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Adjoint (reverse-mode) step, REAL and COMPLEX.  New: the reference has no
+ * adjoint; this differentiates its step (lfm/core/backends/numpy_backend.py:
+ * 80-205) as written, in the reference representation of the state (A/B
+ * buffers, P_prev' = (1-mask) P).  Inputs: the state the step read (psi_r,
+ * psi_i, chi), chi after the step (chi_next, for the clamp at -chi0) and
+ * g_out[6], the adjoints of the step's outputs in the order (psi_r,
+ * psi_r_prev, psi_i, psi_i_prev, chi, chi_prev).  Writes g_in[6], the
+ * adjoints of its inputs in the same order (entries 2 and 3 unused, may be
+ * NULL, at the REAL level).  g_in must not overlap any input.  float32
+ * arithmetic; kappa etc. as in lfm_leapfrog_*_f32.
+ * ------------------------------------------------------------------------ */
+int lfm_adjoint_step_f32(int level, const float* psi_r, const float* psi_i, const float* chi,
+                         const float* chi_next, const float* mask_table, const lfm_mask_lut* lut,
+                         const float* const* g_out, float* const* g_in, int N, double dt2,
+                         double kappa, double lambda_self, double chi0, double e0_sq,
+                         double epsilon_w, void* stream);
+
+/* ------------------------------------------------------------------------
  * Batches of independent lattices (the runs lfm/sweep.py:14-157 makes one
  * Simulation at a time), stepped together: one launch per step, persistent
  * CTAs taking (lattice, row tile, plane chunk) items from a work list sorted

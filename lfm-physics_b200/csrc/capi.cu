@@ -488,6 +488,45 @@ int lfm_leapfrog_complex_f32(const float* psi_r, float* psi_r_prev_io, const flo
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
+int lfm_adjoint_step_f32(int level, const float* psi_r, const float* psi_i, const float* chi,
+                         const float* chi_next, const float* mask_table, const lfm_mask_lut* lut,
+                         const float* const* g_out, float* const* g_in, int N, double dt2,
+                         double kappa, double lambda_self, double chi0, double e0_sq,
+                         double epsilon_w, void* stream) {
+  if (level != LFM_REAL && level != LFM_COMPLEX)
+    return fail(LFM_ERR_UNSUPPORTED, "adjoint step: level %d (REAL and COMPLEX only)", level);
+  int rc = check_n(N);
+  if (rc) return rc;
+  const bool cx = level == LFM_COMPLEX;
+  if (!psi_r || !chi || !chi_next || !g_out || !g_in || (cx && !psi_i))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  for (int f = 0; f < 6; ++f) {
+    const bool need = cx || (f != 2 && f != 3);
+    if (need && (!g_out[f] || !g_in[f]))
+      return fail(LFM_ERR_INVALID_ARG, "adjoint buffer %d is null", f);
+  }
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  std::vector<Span> ins = {{psi_r, b}, {chi, b}, {chi_next, b}};
+  std::vector<Span> outs;
+  if (cx) ins.push_back({psi_i, b});
+  for (int f = 0; f < 6; ++f) {
+    if (!cx && (f == 2 || f == 3)) continue;
+    ins.push_back({g_out[f], b});
+    outs.push_back({g_in[f], b});
+  }
+  rc = check_disjoint(ins, outs);
+  if (rc) return rc;
+  const lfm::StepConsts c =
+      lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, 0, 0, 0, 0);
+  cudaError_t e = lfm::launch_adjoint_step(level, N, psi_r, psi_i, chi, chi_next,
+                                           device_lut(mask_table, lut), g_out, g_in, c,
+                                           static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "adjoint step launch");
+  return LFM_OK;
+}
+
 int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
                            float* psi_i_prev_io, const float* chi, float* chi_prev_io,
                            const float* mask_table, const lfm_mask_lut* lut, int damp_prev,

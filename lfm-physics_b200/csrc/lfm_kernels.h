@@ -50,4 +50,11 @@ cudaError_t launch_helmholtz_multiply_gd(float2* spec, int N, double gamma, doub
                                          cudaStream_t stream);
 cudaError_t launch_clip(const float* in, float* out, int64_t count, cudaStream_t stream);
 
+// Adjoint step (adjoint.cu).  g_out / g_in: adjoints of (psi_r, psi_r_prev,
+// psi_i, psi_i_prev, chi, chi_prev) after / before the step.
+cudaError_t launch_adjoint_step(int level, int N, const float* pr, const float* pi,
+                                const float* chi, const float* chi_next, const MaskLut& lut,
+                                const float* const g_out[6], float* const g_in[6],
+                                const StepConsts& c, cudaStream_t stream);
+
 }  // namespace lfm

@@ -1,0 +1,330 @@
+"""Reverse-mode gradients through many leapfrog steps (REAL and COMPLEX).
+
+``leapfrog(config, state, steps)`` advances a state given in the reference
+representation -- the six arrays (psi_r, psi_r_prev, psi_i, psi_i_prev, chi,
+chi_prev) that one step of lfm/core/backends/numpy_backend.py:80-205 reads
+and writes -- and is differentiable with ``torch.autograd``:
+
+* forward: the resident fused steps (lfm_leapfrog_*_f32), keeping a copy of
+  the state every ``every`` steps (default ceil(sqrt(steps)));
+* backward: segment by segment from the last, the segment's states are
+  recomputed from its checkpoint (bit-identical to the forward run) and the
+  hand-written adjoint step (lfm_adjoint_step_f32) carries the gradient back
+  through each step.
+
+Memory: ceil(steps/every) checkpoints of 4 (REAL) or 6 (COMPLEX) fields plus
+every+1 recomputed states of 2 or 3 fields, instead of all `steps` states.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import torch
+
+from . import _lib
+from .backend import B200Backend, _stream_handle, get_backend
+from .config import FieldLevel
+from .mask import MaskTable
+
+FIELDS = ("psi_r", "psi_r_prev", "psi_i", "psi_i_prev", "chi", "chi_prev")
+
+
+class _Lattice:
+    """Resident slots of one lattice plus the calls that step and un-step it."""
+
+    def __init__(self, config, backend: B200Backend) -> None:
+        self.config = config
+        self.backend = backend
+        self.device = backend.device
+        self.level = FieldLevel(int(config.field_level))
+        if self.level == FieldLevel.COLOR:
+            raise ValueError("the adjoint covers the REAL and COMPLEX levels")
+        self.N = int(config.grid_size)
+        self.n = self.N**3
+        self.cx = self.level == FieldLevel.COMPLEX
+        t = MaskTable.for_lattice(self.N, config.boundary_fraction)
+        self.table = t.to_device(self.device)
+        self.desc = t.desc
+        self.absorb = 1.0 - t.device_mask(self.device)
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.pr = [torch.empty(self.n, **f32) for _ in range(2)]
+        self.pi = [torch.empty(self.n, **f32) for _ in range(2)] if self.cx else None
+        self.chi = [torch.empty(self.n, **f32) for _ in range(2)]
+        self.cur = 0
+        self.damp = False
+        c = config
+        self.common = (float(c.dt) ** 2, float(c.kappa), float(c.lambda_self), float(c.chi0),
+                       float(c.e0_sq))
+
+    # state in the reference representation <-> resident slots
+    def load(self, state) -> None:
+        self.cur, self.damp = 0, False  # prev slots hold the reference prev (already damped)
+        self.pr[0].copy_(state[0].reshape(-1))
+        self.pr[1].copy_(state[1].reshape(-1))
+        if self.cx:
+            self.pi[0].copy_(state[2].reshape(-1))
+            self.pi[1].copy_(state[3].reshape(-1))
+        self.chi[0].copy_(state[4].reshape(-1))
+        self.chi[1].copy_(state[5].reshape(-1))
+
+    def state(self) -> list:
+        c, p = self.cur, 1 - self.cur
+        damp = (lambda t: t * self.absorb) if self.damp else (lambda t: t.clone())  # noqa: E731
+        out = [self.pr[c].clone(), damp(self.pr[p]), None, None, self.chi[c].clone(),
+               self.chi[p].clone()]
+        if self.cx:
+            out[2], out[3] = self.pi[c].clone(), damp(self.pi[p])
+        return out
+
+    def step(self) -> None:
+        c, p = self.cur, 1 - self.cur
+        stream = _stream_handle(self.device)
+        tab, desc = self.table.data_ptr(), ctypes.byref(self.desc)
+        if self.cx:
+            _lib.call("lfm_leapfrog_complex_f32", self.pr[c].data_ptr(), self.pr[p].data_ptr(),
+                      self.pi[c].data_ptr(), self.pi[p].data_ptr(), self.chi[c].data_ptr(),
+                      self.chi[p].data_ptr(), tab, desc, int(self.damp), self.N, *self.common,
+                      float(self.config.epsilon_w), stream)
+        else:
+            _lib.call("lfm_leapfrog_real_f32", self.pr[c].data_ptr(), self.pr[p].data_ptr(),
+                      self.chi[c].data_ptr(), self.chi[p].data_ptr(), tab, desc, int(self.damp),
+                      self.N, *self.common, stream)
+        self.cur = p
+        self.damp = True
+
+    def adjoint_step(self, pr, pi, chi, chi_next, g_out, g_in) -> None:
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        go = (ctypes.c_void_p * 6)(*[ptr(t) for t in g_out])
+        gi = (ctypes.c_void_p * 6)(*[ptr(t) for t in g_in])
+        _lib.call("lfm_adjoint_step_f32", int(self.level), pr.data_ptr(), ptr(pi),
+                  chi.data_ptr(), chi_next.data_ptr(), self.table.data_ptr(),
+                  ctypes.byref(self.desc), go, gi, self.N, *self.common,
+                  float(self.config.epsilon_w), _stream_handle(self.device))
+
+
+class _Plan:
+    """Buffers and captured CUDA graphs of one (steps, every) schedule.
+
+    The first forward / backward of a plan runs eagerly and then captures
+    itself; later calls replay one graph each (all buffers stay put).
+    """
+
+    def __init__(self, lat: _Lattice, steps: int, every: int) -> None:
+        self.lat, self.steps, self.every = lat, steps, every
+        n = lat.n
+        f32 = dict(dtype=torch.float32, device=lat.device)
+        nslots = 6 if lat.cx else 4
+        self.snaps = [[torch.empty(n, **f32) for _ in range(nslots)]
+                      for _ in range(math.ceil(steps / every))]
+        self.meta = [None] * len(self.snaps)
+        self.seg = [[torch.empty(n, **f32) for _ in range(3 if lat.cx else 2)]
+                    for _ in range(every + 1)]
+        self.g = [[None if (not lat.cx and f in (2, 3)) else torch.zeros(n, **f32)
+                   for f in range(6)] for _ in range(2)]
+        self.fwd_graph = None
+        self.bwd_graph = None
+        self.busy = False
+
+    # ---- bodies (run eagerly or under capture) ----
+    def _slots(self):
+        lat = self.lat
+        return [*lat.pr, *lat.chi, *(lat.pi or ())]
+
+    def forward_body(self) -> None:
+        lat = self.lat
+        lat.cur, lat.damp = 0, False
+        for t in range(self.steps):
+            if t % self.every == 0:
+                k = t // self.every
+                for d, src in zip(self.snaps[k], self._slots()):
+                    d.copy_(src)
+                self.meta[k] = (lat.cur, lat.damp)
+            lat.step()
+
+    def backward_body(self) -> int:
+        """Adjoint from g[0]; returns the index of the buffer set holding the result."""
+        lat, every, steps = self.lat, self.every, self.steps
+        cur = 0
+        for si in range(len(self.snaps) - 1, -1, -1):
+            s0 = si * every
+            e0 = min(s0 + every, steps)
+            for d, src in zip(self._slots(), self.snaps[si]):
+                d.copy_(src)
+            lat.cur, lat.damp = self.meta[si]
+
+            def keep(slot):
+                c = lat.cur
+                self.seg[slot][0].copy_(lat.pr[c])
+                self.seg[slot][-1].copy_(lat.chi[c])
+                if lat.cx:
+                    self.seg[slot][1].copy_(lat.pi[c])
+
+            keep(0)
+            for t in range(s0, e0):
+                lat.step()
+                keep(t - s0 + 1)
+            for t in range(e0 - 1, s0 - 1, -1):
+                st, nx = self.seg[t - s0], self.seg[t - s0 + 1]
+                lat.adjoint_step(st[0], st[1] if lat.cx else None, st[-1], nx[-1],
+                                 self.g[cur], self.g[1 - cur])
+                cur = 1 - cur
+        return cur
+
+    # ---- drivers ----
+    def run_forward(self) -> None:
+        if self.fwd_graph is not None:
+            self.fwd_graph.replay()
+            self.lat.cur, self.lat.damp = self._fwd_end
+            return
+        self.forward_body()
+        self._fwd_end = (self.lat.cur, self.lat.damp)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.forward_body()
+        self.fwd_graph = g
+
+    def run_backward(self) -> int:
+        if self.bwd_graph is not None:
+            self.bwd_graph.replay()
+            return self._bwd_out
+        self._bwd_out = self.backward_body()
+        # capture overwrites nothing: the result is already in g[_bwd_out]
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.backward_body()
+        self.bwd_graph = g
+        return self._bwd_out
+
+
+class LeapfrogFunction(torch.autograd.Function):
+    """(psi_r, psi_r_prev, psi_i, psi_i_prev, chi, chi_prev) -> the same after `steps` steps.
+
+    At the REAL level psi_i / psi_i_prev are passed as None and come back None.
+    """
+
+    @staticmethod
+    def forward(ctx, plan: _Plan, *state):
+        lat = plan.lat
+        plan.busy = True
+        lat.load([s.detach() if s is not None else None for s in state])
+        plan.run_forward()
+        ctx.plan = plan
+        out = lat.state()
+        return tuple(None if o is None else o.reshape(lat.N, lat.N, lat.N) for o in out)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        plan = ctx.plan
+        lat = plan.lat
+        g0 = plan.g[0]
+        for f in range(6):
+            if g0[f] is None:
+                continue
+            if grads[f] is None:
+                g0[f].zero_()
+            else:
+                g0[f].copy_(grads[f].reshape(-1))
+        res = plan.run_backward()
+        out = tuple(None if t is None else t.clone().reshape(lat.N, lat.N, lat.N)
+                    for t in plan.g[res])
+        plan.busy = False
+        ctx.plan = None
+        return (None,) + out
+
+
+_LATTICES: dict = {}
+
+
+def _lattice_for(config, be: B200Backend) -> _Lattice:
+    c = config
+    key = (str(be.device), int(c.grid_size), int(c.field_level), float(c.boundary_fraction),
+           float(c.dt), float(c.kappa), float(c.lambda_self), float(c.chi0), float(c.e0_sq),
+           float(c.epsilon_w))
+    lat = _LATTICES.get(key)
+    if lat is None:
+        lat = _LATTICES[key] = _Lattice(config, be)
+        lat.plans = {}
+    return lat
+
+
+def _plan_for(lat: _Lattice, steps: int, every: int) -> _Plan:
+    plan = lat.plans.get((steps, every))
+    if plan is None:
+        plan = lat.plans[(steps, every)] = _Plan(lat, steps, every)
+    if plan.busy:  # a forward whose backward has not run yet holds the cached plan
+        return _Plan(lat, steps, every)
+    return plan
+
+
+def leapfrog(config, state, steps: int, every: int | None = None, backend="auto"):
+    """Differentiable `steps` leapfrog steps of a REAL/COMPLEX state.
+
+    state: six tensors (N, N, N) float32 on the device in the reference
+    representation (psi_i, psi_i_prev None at the REAL level).  Returns the
+    six tensors after the steps.  every: steps between checkpoints
+    (default ceil(sqrt(steps))).  Buffers and CUDA graphs are cached per
+    lattice and schedule, so repeated calls (an optimisation loop) replay
+    one graph for the forward and one for the backward.
+    """
+    be = backend if isinstance(backend, B200Backend) else get_backend(backend)
+    lat = _lattice_for(config, be)
+    steps = int(steps)
+    if steps < 1:
+        raise ValueError("steps must be >= 1")
+    every = int(every or math.ceil(math.sqrt(steps)))
+    every = max(1, min(every, steps))
+    if (state[2] is None) == lat.cx:
+        raise ValueError("psi_i / psi_i_prev must be given exactly at the COMPLEX level")
+    needs_grad = torch.is_grad_enabled() and any(
+        s is not None and s.requires_grad for s in state)
+    if not needs_grad:
+        lat.load(state)
+        for _ in range(steps):
+            lat.step()
+        return tuple(None if o is None else o.reshape(lat.N, lat.N, lat.N) for o in lat.state())
+    return LeapfrogFunction.apply(_plan_for(lat, steps, every), *state)
+
+
+def memory_bytes(config, steps: int, every: int | None = None) -> dict:
+    """Device bytes the checkpoints and the segment buffer of leapfrog() take."""
+    n = int(config.grid_size) ** 3
+    cx = int(config.field_level) == FieldLevel.COMPLEX
+    every = int(every or math.ceil(math.sqrt(steps)))
+    snaps = math.ceil(steps / every)
+    per_snap = (6 if cx else 4) * 4 * n
+    seg = (every + 1) * (3 if cx else 2) * 4 * n
+    return {"checkpoints": snaps, "checkpoint_bytes": snaps * per_snap, "segment_bytes": seg,
+            "all_states_bytes": steps * (3 if cx else 2) * 4 * n}
+
+
+# ------------------------------------------------------------------ initial states
+def soliton_state(N: int, amplitude, centre, phase, sigma: float, chi0: float, dchi=None,
+                  complex_level: bool = True, device=None, dtype=torch.float32):
+    """Differentiable initial state: a sum of Gaussian packets.
+
+    amplitude (S,), centre (S, 3), phase (S,) tensors; packet s is
+    amplitude_s exp(-|x - centre_s|^2 / (2 sigma^2)) e^{i phase_s} (as
+    lfm/fields/soliton.py:49-59 builds them, without wrap).  chi = chi0 +
+    dchi.  Previous fields equal the current ones, as set_psi_real /
+    set_chi leave them.  Returns the six state tensors.
+    """
+    dev = device if device is not None else amplitude.device
+    x = torch.arange(N, device=dev, dtype=dtype)
+    pr = torch.zeros((N, N, N), device=dev, dtype=dtype)
+    pi = torch.zeros((N, N, N), device=dev, dtype=dtype)
+    for s in range(amplitude.shape[0]):
+        c = centre[s].to(dtype)
+        d2 = ((x - c[0]) ** 2)[:, None, None] + ((x - c[1]) ** 2)[None, :, None] \
+            + ((x - c[2]) ** 2)[None, None, :]
+        env = amplitude[s].to(dtype) * torch.exp(-d2 / (2.0 * sigma * sigma))
+        th = phase[s].to(dtype)
+        pr = pr + env * torch.cos(th)
+        pi = pi + env * torch.sin(th)
+    chi = torch.full((N, N, N), float(chi0), device=dev, dtype=dtype)
+    if dchi is not None:
+        chi = chi + dchi.to(dtype)
+    if complex_level:
+        return [pr, pr, pi, pi, chi, chi]
+    return [pr, pr, None, None, chi, chi]
