@@ -188,6 +188,18 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
                                   double dt2, double kappa, double lambda_self, double chi0,
                                   double e0_sq, double epsilon_w, void* stream);
 
+/* Out-of-place form of lfm_leapfrog_real_f32 / lfm_leapfrog_complex_f32
+ * (level LFM_REAL or LFM_COMPLEX): the same step and the same bits, with the
+ * new fields written to *_out instead of over the previous ones, which stay
+ * read-only.  The outputs must not overlap any input.  psi_i* are ignored
+ * (may be NULL) at the REAL level. */
+int lfm_advance_f32(int level, const float* psi_r, const float* psi_r_prev, float* psi_r_out,
+                    const float* psi_i, const float* psi_i_prev, float* psi_i_out,
+                    const float* chi, const float* chi_prev, float* chi_out,
+                    const float* mask_table, const lfm_mask_lut* lut, int damp_prev, int N,
+                    double dt2, double kappa, double lambda_self, double chi0, double e0_sq,
+                    double epsilon_w, void* stream);
+
 /* ------------------------------------------------------------------------
  * Adjoint (reverse-mode) step, REAL and COMPLEX.  New: the reference has no
  * adjoint; this differentiates its step (lfm/core/backends/numpy_backend.py:
@@ -210,8 +222,8 @@ int lfm_adjoint_step_f32(int level, const float* psi_r, const float* psi_i, cons
  * Batches of independent lattices (the runs lfm/sweep.py:14-157 makes one
  * Simulation at a time), stepped together: one launch per step, persistent
  * CTAs taking (lattice, row tile, plane chunk) items from a work list sorted
- * by cost (REAL and COMPLEX items on two groups of CTAs sized by the bytes
- * each level moves), each item marched like the fused single-lattice kernel.  REAL and
+ * by cost (all REAL items, then all COMPLEX ones), each item marched like the
+ * fused single-lattice kernel.  REAL and
  * COMPLEX lattices, N a multiple of 4, any mix of sizes and parameters.  Each
  * lattice keeps two slots per field in the resident layout of
  * lfm_leapfrog_*_f32: at parity p, slot p holds the current fields and slot
@@ -246,15 +258,13 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
                      const lfm_batch_tuning* tuning, lfm_batch** out);
 /* One step of every lattice (one kernel launch). */
 int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream);
-/* Launch shape: work items, CTA size, persistent CTAs, dynamic shared memory,
- * and how many of the CTAs run the REAL items (the rest run COMPLEX). */
-int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem,
-                   int* real_ctas);
+/* Launch shape: work items, CTA size, persistent CTAs, dynamic shared memory. */
+int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem);
 int lfm_batch_destroy(lfm_batch* batch);
 /* The plan lfm_batch_create would make, on the host only (no device needed;
  * 128 registers per thread and `sms` SMs assumed, 148 when sms <= 0).
  * items_out: 6 int32 per item (level, lattice, j0, j1, i0, i1) in the order
- * CTAs take them (REAL first); launch_out: (threads, smem, grid, real_ctas).
+ * CTAs take them (REAL first); launch_out: (threads, smem, grid).
  * Either may be NULL;
  * nitems_out gets the item count. */
 int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_tuning* tuning,

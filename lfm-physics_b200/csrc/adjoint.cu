@@ -48,104 +48,126 @@ struct AdjArgs {
   int use_lambda;
 };
 
-struct Nb {
-  int di, dj, dk;
-  float w;   // Laplacian weight
-  int axis;  // face neighbours: 0, 1, 2; edges: -1
-  float sign;
-};
-
-// The 18 neighbours: 6 faces (1/3) then 12 edges (1/6).
-__constant__ Nb kNb[18] = {
-    {-1, 0, 0, 1.0f / 3.0f, 0, -1.0f}, {1, 0, 0, 1.0f / 3.0f, 0, 1.0f},
-    {0, -1, 0, 1.0f / 3.0f, 1, -1.0f}, {0, 1, 0, 1.0f / 3.0f, 1, 1.0f},
-    {0, 0, -1, 1.0f / 3.0f, 2, -1.0f}, {0, 0, 1, 1.0f / 3.0f, 2, 1.0f},
-    {-1, -1, 0, 1.0f / 6.0f, -1, 0.0f}, {-1, 1, 0, 1.0f / 6.0f, -1, 0.0f},
-    {1, -1, 0, 1.0f / 6.0f, -1, 0.0f},  {1, 1, 0, 1.0f / 6.0f, -1, 0.0f},
-    {-1, 0, -1, 1.0f / 6.0f, -1, 0.0f}, {-1, 0, 1, 1.0f / 6.0f, -1, 0.0f},
-    {1, 0, -1, 1.0f / 6.0f, -1, 0.0f},  {1, 0, 1, 1.0f / 6.0f, -1, 0.0f},
-    {0, -1, -1, 1.0f / 6.0f, -1, 0.0f}, {0, -1, 1, 1.0f / 6.0f, -1, 0.0f},
-    {0, 1, -1, 1.0f / 6.0f, -1, 0.0f},  {0, 1, 1, 1.0f / 6.0f, -1, 0.0f},
-};
-
-__device__ __forceinline__ int wrap(int x, int N) { return x < 0 ? x + N : (x >= N ? x - N : x); }
-
-// a, u_r, u_i and gXn of cell (i, j, k).
-struct Point {
-  float a, ur, ui, gx;
-};
+// ---- tiled kernel ----------------------------------------------------------
+// A CTA owns a TI x TJ x TK block of cells.  Phase 1 evaluates, once per
+// point of the block and its one-cell halo, everything the transposed
+// stencils need from a neighbour (a*gP', a*gX'*[not clamped], and at the
+// COMPLEX level Pr, Pi, w*Pr, w*Pi), into shared memory.  Phase 2 applies
+// the stencils from shared memory.  Threads run along k (coalesced loads,
+// conflict-free shared-memory rows).
+constexpr int TI = 4, TJ = 8, TK = 32;
+constexpr int HI = TI + 2, HJ = TJ + 2, HK = TK + 2;
+constexpr int HALO = HI * HJ * HK;
+constexpr int kThreads = TJ * TK;  // 256: one (j, k) column of TI cells each
 
 template <int LEVEL>
-__device__ __forceinline__ Point point(const AdjArgs& A, int i, int j, int k, int64_t y) {
-  const float m = mask_from_q_flat(A.lut, qterm(i, A.N) + qterm(j, A.N) + qterm(k, A.N));
-  Point p;
-  p.a = fsub(1.0f, m);
-  // the clamp value the forward writes: mask*chi0 + a*(-chi0)
-  const float clamped = fadd(fmul(m, A.chi0), fmul(p.a, A.neg_chi0));
-  const bool live = __ldg(A.chi_next + y) != clamped;
-  p.gx = live ? p.a * __ldg(A.g_chi + y) : 0.0f;
-  p.ur = p.a * __ldg(A.g_pr + y);
-  p.ui = (LEVEL == LFM_COMPLEX) ? p.a * __ldg(A.g_pi + y) : 0.0f;
-  return p;
+struct TileSmem {
+  static constexpr int NF = (LEVEL == LFM_COMPLEX) ? 7 : 2;
+  float f[NF][HALO];  // ur, gx [, ui, pr, pi, wpr, wpi]
+};
+
+__device__ __forceinline__ int wrapmod(int x, int N) {
+  x %= N;
+  return x < 0 ? x + N : x;
 }
 
 template <int LEVEL>
-__global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjArgs A) {
+__global__ void __launch_bounds__(kThreads) adjoint_tile_kernel(const AdjArgs A) {
+  extern __shared__ __align__(16) float sm_raw[];
+  TileSmem<LEVEL>& S = *reinterpret_cast<TileSmem<LEVEL>*>(sm_raw);
   const int N = A.N;
-  const int64_t n3 = (int64_t)N * N * N;
+  const int tiles_k = (N + TK - 1) / TK, tiles_j = (N + TJ - 1) / TJ;
+  int t = blockIdx.x;
+  const int k0 = (t % tiles_k) * TK;
+  t /= tiles_k;
+  const int j0 = (t % tiles_j) * TJ;
+  const int i0 = (t / tiles_j) * TI;
   const float c_w = -0.5f * A.eps_w * A.K * A.dt2;  // w(y) = c_w X(y) gXn(y)
-  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n3;
-       x += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(x % N);
-    const int j = (int)((x / N) % N);
-    const int i = (int)(x / ((int64_t)N * N));
-    const Point p0 = point<LEVEL>(A, i, j, k, x);
-    float lapR = -4.0f * p0.ur, lapI = -4.0f * p0.ui, lapX = -4.0f * p0.gx;
-    float dPr = 0.0f, dPi = 0.0f, dwPr = 0.0f, dwPi = 0.0f;
+
+  // phase 1: point terms of the block and its halo
+  for (int h = threadIdx.x; h < HALO; h += kThreads) {
+    const int hk = h % HK, hj = (h / HK) % HJ, hi = h / (HK * HJ);
+    const int gi = wrapmod(i0 + hi - 1, N), gj = wrapmod(j0 + hj - 1, N),
+              gk = wrapmod(k0 + hk - 1, N);
+    const int64_t y = ((int64_t)gi * N + gj) * N + gk;
+    const float m = mask_from_q_flat(A.lut, qterm(gi, N) + qterm(gj, N) + qterm(gk, N));
+    const float a = fsub(1.0f, m);
+    // the clamp value the forward writes: mask*chi0 + a*(-chi0)
+    const float clamped = fadd(fmul(m, A.chi0), fmul(a, A.neg_chi0));
+    const float gx = (__ldg(A.chi_next + y) != clamped) ? a * __ldg(A.g_chi + y) : 0.0f;
+    S.f[0][h] = a * __ldg(A.g_pr + y);
+    S.f[1][h] = gx;
+    if constexpr (LEVEL == LFM_COMPLEX) {
+      const float pr = __ldg(A.pr + y), pi = __ldg(A.pi + y);
+      const float w = c_w * __ldg(A.chi + y) * gx;
+      S.f[2][h] = a * __ldg(A.g_pi + y);
+      S.f[3][h] = pr;
+      S.f[4][h] = pi;
+      S.f[5][h] = w * pr;
+      S.f[6][h] = w * pi;
+    }
+  }
+  __syncthreads();
+
+  // phase 2: one (j, k) column of TI cells per thread
+  const int tk = threadIdx.x % TK, tj = threadIdx.x / TK;
+  const int gj = j0 + tj, gk = k0 + tk;
+  if (gj >= N || gk >= N) return;
+  constexpr int DI = HJ * HK, DJ = HK;
+  const float third = 1.0f / 3.0f, sixth = 1.0f / 6.0f;
 #pragma unroll
-    for (int q = 0; q < 18; ++q) {
-      const Nb nb = kNb[q];
-      const int yi = wrap(i + nb.di, N), yj = wrap(j + nb.dj, N), yk = wrap(k + nb.dk, N);
-      const int64_t y = ((int64_t)yi * N + yj) * N + yk;
-      const Point p = point<LEVEL>(A, yi, yj, yk, y);
-      lapR += nb.w * p.ur;
-      lapX += nb.w * p.gx;
-      if (LEVEL == LFM_COMPLEX) lapI += nb.w * p.ui;
-      if (q < 6 && LEVEL == LFM_COMPLEX) {
-        const float pr = __ldg(A.pr + y), pi = __ldg(A.pi + y);
-        const float wy = c_w * __ldg(A.chi + y) * p.gx;
-        dPr += nb.sign * pr;
-        dPi += nb.sign * pi;
-        dwPr += nb.sign * wy * pr;
-        dwPi += nb.sign * wy * pi;
-      }
-    }
+  for (int ti = 0; ti < TI; ++ti) {
+    const int gi = i0 + ti;
+    if (gi >= N) break;
+    const int64_t x = ((int64_t)gi * N + gj) * N + gk;
+    const int c = ((ti + 1) * HJ + (tj + 1)) * HK + (tk + 1);
+    // transposed (= the) Laplacian of a shared-memory field at the centre
+    auto lap = [&](const float* f) {
+      const float faces = f[c - DI] + f[c + DI] + f[c - DJ] + f[c + DJ] + f[c - 1] + f[c + 1];
+      const float edges = f[c - DI - DJ] + f[c - DI + DJ] + f[c + DI - DJ] + f[c + DI + DJ] +
+                          f[c - DI - 1] + f[c - DI + 1] + f[c + DI - 1] + f[c + DI + 1] +
+                          f[c - DJ - 1] + f[c - DJ + 1] + f[c + DJ - 1] + f[c + DJ + 1];
+      return third * faces + sixth * edges - 4.0f * f[c];
+    };
+    // sum over the axes of f[x + e] - f[x - e]
+    auto dsum = [&](const float* f) {
+      return (f[c + DI] - f[c - DI]) + (f[c + DJ] - f[c - DJ]) + (f[c + 1] - f[c - 1]);
+    };
+    const float ur = S.f[0][c], gx = S.f[1][c];
+    const float lapR = lap(S.f[0]), lapX = lap(S.f[1]);
+    const float m0 = mask_from_q_flat(A.lut, qterm(gi, N) + qterm(gj, N) + qterm(gk, N));
+    const float a0 = fsub(1.0f, m0);
     const float X = __ldg(A.chi + x);
-    const float Pr = __ldg(A.pr + x);
-    const float Pi = (LEVEL == LFM_COMPLEX) ? __ldg(A.pi + x) : 0.0f;
-    float Q;
-    if (LEVEL == LFM_COMPLEX) {
-      const float jt = 0.5f * (Pr * dPi - Pi * dPr);
-      Q = Pr * Pr + Pi * Pi + A.eps_w * jt - A.e0_sq;
-    } else {
-      Q = Pr * Pr - A.e0_sq;
-    }
-    const float gacc = A.dt2 * p0.gx;
-    const float gQ = -gacc * A.K * X;
     const float X2 = X * X;
-    A.o_pr[x] = p0.a * __ldg(A.g_prp + x) + 2.0f * p0.ur + A.dt2 * lapR - A.dt2 * X2 * p0.ur +
-                2.0f * Pr * gQ +
-                ((LEVEL == LFM_COMPLEX) ? (0.5f * A.eps_w * gQ) * dPi + dwPi : 0.0f);
-    A.o_prp[x] = -p0.ur;
-    if (LEVEL == LFM_COMPLEX) {
-      A.o_pi[x] = p0.a * __ldg(A.g_pip + x) + 2.0f * p0.ui + A.dt2 * lapI - A.dt2 * X2 * p0.ui +
-                  2.0f * Pi * gQ - (0.5f * A.eps_w * gQ) * dPr - dwPr;
-      A.o_pip[x] = -p0.ui;
-    }
+    const float gacc = A.dt2 * gx;
+    const float gQ = -gacc * A.K * X;
     const float hp = A.use_lambda ? A.four_lambda * (3.0f * X2 - A.chi0_sq) : 0.0f;
-    A.o_chi[x] = __ldg(A.g_chip + x) + 2.0f * p0.gx + A.dt2 * lapX - gacc * (hp + A.K * Q) -
-                 2.0f * A.dt2 * X * (Pr * p0.ur + Pi * p0.ui);
-    A.o_chip[x] = -p0.gx;
+    if constexpr (LEVEL == LFM_COMPLEX) {
+      const float ui = S.f[2][c], Pr = S.f[3][c], Pi = S.f[4][c];
+      const float lapI = lap(S.f[2]);
+      const float dPr = dsum(S.f[3]), dPi = dsum(S.f[4]);
+      const float dwPr = dsum(S.f[5]), dwPi = dsum(S.f[6]);
+      const float jt = 0.5f * (Pr * dPi - Pi * dPr);
+      const float Q = Pr * Pr + Pi * Pi + A.eps_w * jt - A.e0_sq;
+      const float w0 = 0.5f * A.eps_w * gQ;
+      A.o_pr[x] = a0 * __ldg(A.g_prp + x) + 2.0f * ur + A.dt2 * lapR - A.dt2 * X2 * ur +
+                  2.0f * Pr * gQ + w0 * dPi + dwPi;
+      A.o_pi[x] = a0 * __ldg(A.g_pip + x) + 2.0f * ui + A.dt2 * lapI - A.dt2 * X2 * ui +
+                  2.0f * Pi * gQ - w0 * dPr - dwPr;
+      A.o_prp[x] = -ur;
+      A.o_pip[x] = -ui;
+      A.o_chi[x] = __ldg(A.g_chip + x) + 2.0f * gx + A.dt2 * lapX - gacc * (hp + A.K * Q) -
+                   2.0f * A.dt2 * X * (Pr * ur + Pi * ui);
+    } else {
+      const float E = __ldg(A.pr + x);
+      const float Q = E * E - A.e0_sq;
+      A.o_pr[x] = a0 * __ldg(A.g_prp + x) + 2.0f * ur + A.dt2 * lapR - A.dt2 * X2 * ur +
+                  2.0f * E * gQ;
+      A.o_prp[x] = -ur;
+      A.o_chi[x] = __ldg(A.g_chip + x) + 2.0f * gx + A.dt2 * lapX - gacc * (hp + A.K * Q) -
+                   2.0f * A.dt2 * X * E * ur;
+    }
+    A.o_chip[x] = -gx;
   }
 }
 
@@ -176,14 +198,21 @@ cudaError_t launch_adjoint_step(int level, int N, const float* pr, const float* 
   A.chi0_sq = c.chi0_sq;
   A.neg_chi0 = c.neg_chi0;
   A.use_lambda = c.use_lambda;
-  const int64_t n3 = (int64_t)N * N * N;
-  const int block = 256;
-  int64_t blocks = (n3 + block - 1) / block;
-  if (blocks > 148LL * 16) blocks = 148LL * 16;
-  if (level == LFM_REAL)
-    adjoint_step_kernel<LFM_REAL><<<(int)blocks, block, 0, stream>>>(A);
-  else
-    adjoint_step_kernel<LFM_COMPLEX><<<(int)blocks, block, 0, stream>>>(A);
+  const int tiles = ((N + TK - 1) / TK) * ((N + TJ - 1) / TJ) * ((N + TI - 1) / TI);
+  if (level == LFM_REAL) {
+    const int smem = (int)sizeof(TileSmem<LFM_REAL>);
+    adjoint_tile_kernel<LFM_REAL><<<tiles, kThreads, smem, stream>>>(A);
+  } else {
+    const int smem = (int)sizeof(TileSmem<LFM_COMPLEX>);
+    static bool granted = false;  // 57 KB: above the 48 KB default
+    if (!granted) {
+      cudaError_t e = cudaFuncSetAttribute(adjoint_tile_kernel<LFM_COMPLEX>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      granted = true;
+    }
+    adjoint_tile_kernel<LFM_COMPLEX><<<tiles, kThreads, smem, stream>>>(A);
+  }
   return cudaGetLastError();
 }
 

@@ -488,6 +488,47 @@ int lfm_leapfrog_complex_f32(const float* psi_r, float* psi_r_prev_io, const flo
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
+int lfm_advance_f32(int level, const float* psi_r, const float* psi_r_prev, float* psi_r_out,
+                    const float* psi_i, const float* psi_i_prev, float* psi_i_out,
+                    const float* chi, const float* chi_prev, float* chi_out,
+                    const float* mask_table, const lfm_mask_lut* lut, int damp_prev, int N,
+                    double dt2, double kappa, double lambda_self, double chi0, double e0_sq,
+                    double epsilon_w, void* stream) {
+  if (level != LFM_REAL && level != LFM_COMPLEX)
+    return fail(LFM_ERR_UNSUPPORTED, "advance: level %d (REAL and COMPLEX only)", level);
+  int rc = check_n(N);
+  if (rc) return rc;
+  const bool cx = level == LFM_COMPLEX;
+  if (!psi_r || !psi_r_prev || !psi_r_out || !chi || !chi_prev || !chi_out ||
+      (cx && (!psi_i || !psi_i_prev || !psi_i_out)))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  std::vector<Span> ins = {{psi_r, b}, {psi_r_prev, b}, {chi, b}, {chi_prev, b}};
+  std::vector<Span> outs = {{psi_r_out, b}, {chi_out, b}};
+  if (cx) {
+    ins.push_back({psi_i, b});
+    ins.push_back({psi_i_prev, b});
+    outs.push_back({psi_i_out, b});
+  }
+  rc = check_disjoint(ins, outs);
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = level;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, cx ? epsilon_w : 0.0, 0, 0,
+                              0, 0);
+  a.pr = psi_r; a.pr_prev = psi_r_prev; a.pr_out = psi_r_out;
+  if (cx) {
+    a.pi = psi_i; a.pi_prev = psi_i_prev; a.pi_out = psi_i_out;
+  }
+  a.chi = chi; a.chi_prev = chi_prev; a.chi_out = chi_out;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
 int lfm_adjoint_step_f32(int level, const float* psi_r, const float* psi_i, const float* chi,
                          const float* chi_next, const float* mask_table, const lfm_mask_lut* lut,
                          const float* const* g_out, float* const* g_in, int N, double dt2,
@@ -772,7 +813,7 @@ namespace {
 // (lfm_batch_plan exposes it without a device).
 struct BatchPlan {
   std::vector<lfm::BatchItem> items;  // REAL items, then COMPLEX, each largest first
-  int real_items = 0, real_ctas = 0;
+  int real_items = 0;
   int threads = 0, smem = 0, grid = 0;
   std::vector<int> TJ, IC, stage_floats;
 };
@@ -846,21 +887,16 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
       for (int i0 = 0; i0 < N; i0 += IC)
         plan->items.push_back({l, level, j0, i0, std::min(N, i0 + IC)});
   }
-  // REAL before COMPLEX, largest first within a level: each free CTA of a
-  // level's group takes the next item (longest-processing-time order)
+  // REAL before COMPLEX, largest first within a level: each free CTA takes
+  // the next item (longest-processing-time order)
   std::stable_sort(plan->items.begin(), plan->items.end(),
                    [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
                      if (a.level != b.level) return a.level < b.level;
                      return item_cost(a, plan->TJ[a.lattice], L[a.lattice].N) >
                             item_cost(b, plan->TJ[b.lattice], L[b.lattice].N);
                    });
-  double bytes[2] = {0.0, 0.0};
-  int count_lv[2] = {0, 0};
-  for (const lfm::BatchItem& it : plan->items) {
-    bytes[it.level] += (double)item_cost(it, plan->TJ[it.lattice], L[it.lattice].N);
-    ++count_lv[it.level];
-  }
-  plan->real_items = count_lv[0];
+  plan->real_items = 0;
+  for (const lfm::BatchItem& it : plan->items) plan->real_items += it.level == LFM_REAL;
   plan->threads = threads;
   plan->smem = t.stages * max_stage * (int)sizeof(float);
   if (plan->smem > kBatchSmemLimit)
@@ -870,17 +906,7 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
                          65536 / std::max(1, regs * threads)});
   per_sm = std::max(1, per_sm);
   if (t.ctas_per_sm > 0) per_sm = std::min(per_sm, t.ctas_per_sm);
-  // resident CTAs split between the levels in proportion to the bytes each moves
-  const int G = sms * per_sm;
-  int g_real = 0;
-  if (count_lv[0] && count_lv[1])
-    g_real = std::max(1, std::min(G - 1, (int)std::lround(G * bytes[0] / (bytes[0] + bytes[1]))));
-  else if (count_lv[0])
-    g_real = G;
-  g_real = std::min(g_real, count_lv[0]);
-  const int g_cx = std::min(G - g_real, count_lv[1]);
-  plan->real_ctas = g_real;
-  plan->grid = g_real + g_cx;
+  plan->grid = std::min((int)plan->items.size(), sms * per_sm);
   return LFM_OK;
 }
 
@@ -892,7 +918,7 @@ struct lfm_batch {
   lfm::BatchLattice* d_lat = nullptr;
   lfm::BatchItem* d_items = nullptr;
   int* d_counters = nullptr;  // next REAL item, next COMPLEX item, retired CTAs
-  int nitems = 0, real_items = 0, real_ctas = 0, threads = 0, smem = 0, grid = 0;
+  int nitems = 0, real_items = 0, threads = 0, smem = 0, grid = 0;
 };
 
 extern "C" {
@@ -929,7 +955,6 @@ int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_
     launch_out[0] = plan.threads;
     launch_out[1] = plan.smem;
     launch_out[2] = plan.grid;
-    launch_out[3] = plan.real_ctas;
   }
   return LFM_OK;
 }
@@ -988,7 +1013,6 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
   B->stages = t.stages;
   B->nitems = (int)plan.items.size();
   B->real_items = plan.real_items;
-  B->real_ctas = plan.real_ctas;
   B->threads = plan.threads;
   B->smem = plan.smem;
   B->grid = plan.grid;
@@ -1022,7 +1046,6 @@ int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
   P.items = batch->d_items;
   P.nitems = batch->nitems;
   P.real_items = batch->real_items;
-  P.real_ctas = batch->real_ctas;
   P.parity = parity;
   P.damp_prev = damp_prev ? 1 : 0;
   P.stages = batch->stages;
@@ -1035,10 +1058,8 @@ int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
   return LFM_OK;
 }
 
-int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem,
-                   int* real_ctas) {
+int lfm_batch_info(const lfm_batch* batch, int* items, int* threads, int* grid, int* smem) {
   if (!batch) return fail(LFM_ERR_INVALID_ARG, "null batch");
-  if (real_ctas) *real_ctas = batch->real_ctas;
   if (items) *items = batch->nitems;
   if (threads) *threads = batch->threads;
   if (grid) *grid = batch->grid;

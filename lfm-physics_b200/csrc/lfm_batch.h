@@ -34,7 +34,6 @@ struct BatchParams {
   const BatchItem* items;  // REAL items first, then COMPLEX, each sorted by cost
   int nitems;
   int real_items;  // items[0, real_items) are REAL
-  int real_ctas;   // CTAs [0, real_ctas) run the REAL items
   int parity;     // slot holding the current fields
   int damp_prev;  // previous-field slots hold undamped values
   int stages;

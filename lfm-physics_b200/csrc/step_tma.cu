@@ -911,17 +911,21 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
   }
 }
 
-// CTAs [0, real_ctas) run the REAL items, the others the COMPLEX ones (the
-// split follows the bytes each level moves).
+// Every CTA drains the REAL list, then the COMPLEX list: a CTA done with
+// the REAL items starts on the COMPLEX ones at once, so the launch has a
+// single tail (the smallest COMPLEX items).  The two loops run one after the
+// other, so their register demands do not add up.
 __global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ BatchParams B) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
   __shared__ QShared sh;
   __shared__ TmaParams P;
   __shared__ int s_item;
-  if ((int)blockIdx.x < B.real_ctas)
+  sh.abort_flag = 0;
+  if (B.real_items > 0)
     batch_level<LFM_REAL, 4>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P, s_item);
-  else
+  __syncthreads();
+  if (!sh.abort_flag && B.nitems > B.real_items)
     batch_level<LFM_COMPLEX, 2>(B, B.items + B.real_items, B.nitems - B.real_items,
                                 B.next_item + 1, smem, bars, sh, P, s_item);
   if (threadIdx.x == 0) {
@@ -1001,17 +1005,24 @@ Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threa
   if (forced && forced->ic > 0) {
     best.IC = std::min(forced->ic, N);
   } else {
-    // Planes per chunk: balance the last wave of tiles over 148 SMs against
-    // the two halo planes each chunk loads in addition to its own.
+    // Planes per chunk: minimise waves x (pipeline fill + (IC + 2) planes).
+    // A CTA streams one plane of TJ x N cells in t_plane, no faster than the
+    // ring's S - 2 planes in flight allow; per-SM rates measured at 512^3
+    // (REAL, 0.97 kcell/us) and 256^3 (COMPLEX, 0.46).  Large lattices end up
+    // balancing their last wave, small ones (latency-bound) take short
+    // chunks and many CTAs.
     const double slots = 148.0 * ctas;
-    double best_eff = -1.0;
-    for (int ic = std::min(8, N); ic <= N; ++ic) {
-      const int chunks = (N + ic - 1) / ic;
-      const double waves = (double)JT * chunks / slots;
-      const double fill = waves / std::ceil(waves);
-      const double eff = fill * (double)N / (N + 2.0 * chunks);
-      if (eff > best_eff + 1e-9) {
-        best_eff = eff;
+    const double r_sm = (level == LFM_REAL) ? 0.97e3 : (level == LFM_COMPLEX ? 0.46e3 : 0.2e3);
+    const double t_fill = 2.0, t_lat = 1.5;  // us
+    const double t_plane = std::max((double)best.TJ * N * ctas / r_sm,
+                                    t_lat / std::max(1, best.S - (min_s - 1)));
+    double best_t = 1e300;
+    for (int chunks = 1; chunks <= std::max(1, N / 2); ++chunks) {
+      const int ic = (N + chunks - 1) / chunks;
+      const double waves = std::ceil((double)JT * chunks / slots);
+      const double t = waves * (t_fill + (ic + 2) * t_plane);
+      if (t < best_t * (1.0 - 1e-9)) {
+        best_t = t;
         best.IC = ic;
       }
     }

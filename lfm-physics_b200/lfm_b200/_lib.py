@@ -79,11 +79,13 @@ _SIGNATURES = {
     "lfm_device_status": [POINTER(c_int), c_int],
     "lfm_metrics_f64": [_P, c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
     "lfm_metrics_f64_noalloc": [c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
+    "lfm_advance_f32": [c_int] + [_P] * 10 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6
+    + [_P],
     "lfm_adjoint_step_f32": [c_int] + [_P] * 5 + [POINTER(MaskLut), POINTER(c_void_p),
                                                     POINTER(c_void_p), c_int] + [_D] * 6 + [_P],
     "lfm_batch_create": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), POINTER(c_void_p)],
     "lfm_batch_step": [_P, c_int, c_int, _P],
-    "lfm_batch_info": [_P] + [POINTER(c_int)] * 5,
+    "lfm_batch_info": [_P] + [POINTER(c_int)] * 4,
     "lfm_batch_destroy": [_P],
     "lfm_batch_plan": [POINTER(LatticeDesc), c_int, POINTER(BatchTuning), c_int, POINTER(c_int32),
                        c_int, POINTER(c_int), POINTER(c_int32)],

@@ -13,7 +13,7 @@ and writes -- and is differentiable with ``torch.autograd``:
   through each step.
 
 Memory: ceil(steps/every) checkpoints of 4 (REAL) or 6 (COMPLEX) fields plus
-every+1 recomputed states of 2 or 3 fields, instead of all `steps` states.
+`every` recomputed states of 2 or 3 fields, instead of all `steps` states.
 """
 
 from __future__ import annotations
@@ -94,6 +94,16 @@ class _Lattice:
         self.cur = p
         self.damp = True
 
+    def advance(self, cur, prev, out, damp: bool) -> None:
+        """One step out of place: cur / prev / out are (psi_r, psi_i, chi) triples
+        (psi_i None at REAL); the new fields go to `out` (lfm_advance_f32)."""
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        _lib.call("lfm_advance_f32", int(self.level), cur[0].data_ptr(), prev[0].data_ptr(),
+                  out[0].data_ptr(), ptr(cur[1]), ptr(prev[1]), ptr(out[1]), cur[2].data_ptr(),
+                  prev[2].data_ptr(), out[2].data_ptr(), self.table.data_ptr(),
+                  ctypes.byref(self.desc), int(damp), self.N, *self.common,
+                  float(self.config.epsilon_w), _stream_handle(self.device))
+
     def adjoint_step(self, pr, pi, chi, chi_next, g_out, g_in) -> None:
         ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
         go = (ctypes.c_void_p * 6)(*[ptr(t) for t in g_out])
@@ -115,12 +125,16 @@ class _Plan:
         self.lat, self.steps, self.every = lat, steps, every
         n = lat.n
         f32 = dict(dtype=torch.float32, device=lat.device)
-        nslots = 6 if lat.cx else 4
-        self.snaps = [[torch.empty(n, **f32) for _ in range(nslots)]
-                      for _ in range(math.ceil(steps / every))]
-        self.meta = [None] * len(self.snaps)
-        self.seg = [[torch.empty(n, **f32) for _ in range(3 if lat.cx else 2)]
-                    for _ in range(every + 1)]
+
+        def triple():
+            return [torch.empty(n, **f32), torch.empty(n, **f32) if lat.cx else None,
+                    torch.empty(n, **f32)]
+
+        # checkpoint k: the (current, previous) slot triples before step k*every
+        self.snaps = [(triple(), triple()) for _ in range(math.ceil(steps / every))]
+        self.meta = [False] * len(self.snaps)  # damp flag of each checkpoint
+        # recomputed states 1 .. every of a segment (state 0 is the checkpoint)
+        self.seg = [triple() for _ in range(every)]
         self.g = [[None if (not lat.cx and f in (2, 3)) else torch.zeros(n, **f32)
                    for f in range(6)] for _ in range(2)]
         self.fwd_graph = None
@@ -128,47 +142,41 @@ class _Plan:
         self.busy = False
 
     # ---- bodies (run eagerly or under capture) ----
-    def _slots(self):
-        lat = self.lat
-        return [*lat.pr, *lat.chi, *(lat.pi or ())]
-
     def forward_body(self) -> None:
         lat = self.lat
         lat.cur, lat.damp = 0, False
         for t in range(self.steps):
             if t % self.every == 0:
                 k = t // self.every
-                for d, src in zip(self.snaps[k], self._slots()):
-                    d.copy_(src)
-                self.meta[k] = (lat.cur, lat.damp)
+                cur, prev = self.snaps[k]
+                c, p = lat.cur, 1 - lat.cur
+                for dst, src in ((cur, (lat.pr[c], lat.pi[c] if lat.cx else None, lat.chi[c])),
+                                 (prev, (lat.pr[p], lat.pi[p] if lat.cx else None, lat.chi[p]))):
+                    for d, x in zip(dst, src):
+                        if d is not None:
+                            d.copy_(x)
+                self.meta[k] = lat.damp
             lat.step()
 
     def backward_body(self) -> int:
-        """Adjoint from g[0]; returns the index of the buffer set holding the result."""
+        """Adjoint from g[0]; returns the index of the buffer set holding the result.
+
+        Each segment is recomputed out of place from its checkpoint straight
+        into the segment buffers (no copies), then walked backwards."""
         lat, every, steps = self.lat, self.every, self.steps
         cur = 0
         for si in range(len(self.snaps) - 1, -1, -1):
             s0 = si * every
             e0 = min(s0 + every, steps)
-            for d, src in zip(self._slots(), self.snaps[si]):
-                d.copy_(src)
-            lat.cur, lat.damp = self.meta[si]
-
-            def keep(slot):
-                c = lat.cur
-                self.seg[slot][0].copy_(lat.pr[c])
-                self.seg[slot][-1].copy_(lat.chi[c])
-                if lat.cx:
-                    self.seg[slot][1].copy_(lat.pi[c])
-
-            keep(0)
+            c0, p0 = self.snaps[si]
+            states = [c0] + self.seg[: e0 - s0]
             for t in range(s0, e0):
-                lat.step()
-                keep(t - s0 + 1)
+                u = t - s0
+                lat.advance(states[u], p0 if u == 0 else states[u - 1], states[u + 1],
+                            self.meta[si] if u == 0 else True)
             for t in range(e0 - 1, s0 - 1, -1):
-                st, nx = self.seg[t - s0], self.seg[t - s0 + 1]
-                lat.adjoint_step(st[0], st[1] if lat.cx else None, st[-1], nx[-1],
-                                 self.g[cur], self.g[1 - cur])
+                st, nx = states[t - s0], states[t - s0 + 1]
+                lat.adjoint_step(st[0], st[1], st[2], nx[2], self.g[cur], self.g[1 - cur])
                 cur = 1 - cur
         return cur
 
@@ -294,7 +302,7 @@ def memory_bytes(config, steps: int, every: int | None = None) -> dict:
     every = int(every or math.ceil(math.sqrt(steps)))
     snaps = math.ceil(steps / every)
     per_snap = (6 if cx else 4) * 4 * n
-    seg = (every + 1) * (3 if cx else 2) * 4 * n
+    seg = every * (3 if cx else 2) * 4 * n
     return {"checkpoints": snaps, "checkpoint_bytes": snaps * per_snap, "segment_bytes": seg,
             "all_states_bytes": steps * (3 if cx else 2) * 4 * n}
 

@@ -71,6 +71,29 @@ def _time_ms(device, fn, steps: int) -> float:
     return a.elapsed_time(b) / steps
 
 
+def _time_graph_ms(evolver, steps: int) -> float:
+    """Device time per step of `steps` (even) resident steps replayed as one
+    CUDA graph, so that host launch overhead does not hide small lattices'
+    kernel time."""
+    import torch
+
+    steps += steps % 2
+    evolver._step()  # first launch of this tile outside capture (and prev damped)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        for _ in range(steps):
+            evolver._step()
+    g.replay()
+    torch.cuda.synchronize(evolver.device)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    g.replay()
+    b.record()
+    torch.cuda.synchronize(evolver.device)
+    return a.elapsed_time(b) / steps
+
+
 # ------------------------------------------------------------------ batches
 BATCH_CANDIDATES = [
     dict(threads=t, stages=s, item_cells=c)
@@ -121,9 +144,13 @@ def tune_batch(batch, candidates=None, steps: int = 6, use_cache: bool = True) -
 
 # ------------------------------------------------------------------ one lattice
 def lattice_candidates(level: int):
+    """Vector width x rows per tile x stages x plane chunk (0 = the planner's
+    wave-balanced chunk).  Small lattices are latency-bound: deep rings and
+    short chunks (many CTAs, few planes each) pay there."""
     vecs = (4, 2) if level == 0 else (2,)
     return [dict(vec=v, tj=tj, stages=s, ic=ic)
-            for v, tj, s, ic in itertools.product(vecs, (1, 2, 4, 8), (3, 4), (0, 32, 64))]
+            for v, tj, s, ic in itertools.product(vecs, (1, 2, 4, 8), (3, 4, 6),
+                                                  (0, 4, 8, 16, 32, 64))]
 
 
 def tune_lattice(evolver, candidates=None, steps: int = 20, use_cache: bool = True) -> dict:
@@ -150,8 +177,7 @@ def tune_lattice(evolver, candidates=None, steps: int = 20, use_cache: bool = Tr
             _lib.tune_set(level, N, cand["tj"], cand["stages"], cand["ic"], cand["vec"])
             evolver._graphs = {}
             try:
-                ms = _time_ms(evolver.device, lambda k: [evolver._step() for _ in range(k)],
-                              steps)
+                ms = _time_graph_ms(evolver, steps)
             except _lib.LfmError:
                 continue  # tile does not fit this N
             used = _lib.tune_get(level, N)

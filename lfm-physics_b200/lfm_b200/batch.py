@@ -148,11 +148,10 @@ class BatchedLattices:
 
     # ---------------------------------------------------------------- plan
     def info(self) -> dict:
-        """Launch shape: work items, threads per CTA, persistent CTAs, shared memory,
-        CTAs of the REAL group."""
-        v = [ctypes.c_int(0) for _ in range(5)]
+        """Launch shape: work items, threads per CTA, persistent CTAs, shared memory."""
+        v = [ctypes.c_int(0) for _ in range(4)]
         _lib.call("lfm_batch_info", self._handle, *[ctypes.byref(x) for x in v])
-        return dict(zip(("items", "threads", "grid", "smem", "real_ctas"), (x.value for x in v)))
+        return dict(zip(("items", "threads", "grid", "smem"), (x.value for x in v)))
 
     # ---------------------------------------------------------------- stepping
     def _step(self) -> None:
@@ -337,7 +336,7 @@ def plan(configs, tuning: dict | None = None, sms: int = 148) -> dict:
     """The work list lfm_batch_create would build for these configs (host only, no device).
 
     Returns {"items": int32 array (n, 6) of (level, lattice, j0, j1, i0, i1),
-    "launch": (threads, smem, grid, real_ctas)}.
+    "launch": (threads, smem, grid)}.
     """
     descs = (_lib.LatticeDesc * len(configs))()
     for i, c in enumerate(configs):
@@ -351,7 +350,7 @@ def plan(configs, tuning: dict | None = None, sms: int = 148) -> dict:
     _lib.check(lib.lfm_batch_plan(descs, len(configs), ctypes.byref(t), int(sms), None, 0,
                                   ctypes.byref(n), None), "lfm_batch_plan")
     items = np.zeros((max(n.value, 1), 6), dtype=np.int32)
-    launch = np.zeros(4, dtype=np.int32)
+    launch = np.zeros(3, dtype=np.int32)
     i32p = ctypes.POINTER(ctypes.c_int32)
     _lib.check(lib.lfm_batch_plan(descs, len(configs), ctypes.byref(t), int(sms),
                                   items.ctypes.data_as(i32p), items.shape[0], ctypes.byref(n),

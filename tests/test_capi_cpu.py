@@ -42,6 +42,28 @@ def test_library_exports_every_declared_function(lib):
     assert lib.lfm_abi_version() == 1
 
 
+def header_arity() -> dict:
+    """Parameter count of every function the header declares."""
+    text = (ROOT / "include" / "lfm_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"^\s*(?:const\s+char\*|int)\s+(lfm_\w+)\s*\(([^;]*?)\)\s*;", text,
+                         re.M | re.S):
+        params = m.group(2).strip()
+        out[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_binding_signatures_match_the_header(lib):
+    from lfm_b200 import _lib
+
+    arity = header_arity()
+    assert len(arity) >= 20
+    for name, args in _lib._SIGNATURES.items():
+        assert name in arity, name
+        assert len(args) == arity[name], (name, len(args), arity[name])
+
+
 def test_strerror_names_codes(lib):
     assert lib.lfm_strerror(0) == b"ok"
     assert lib.lfm_strerror(6).startswith(b"mask")
