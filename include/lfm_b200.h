@@ -188,6 +188,22 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
                                   double dt2, double kappa, double lambda_self, double chi0,
                                   double e0_sq, double epsilon_w, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Poisson equilibration of chi (lfm/fields/equilibrium.py:26-121, as
+ * Simulation.equilibrate calls it, lfm/simulation.py:877-963):
+ * chi = chi0 + dchi with  laplacian(dchi) = kappa (|Psi|^2 - e0_sq)  solved
+ * by FFT on the periodic lattice (DC of dchi = 0); with frozen != 0, chi0 on
+ * the shell dist > N/2 (1 - boundary_fraction) (~interior_mask).  |Psi|^2
+ * sums psi_r^2 (+ psi_i^2), over three colours at the COLOR level (3 N^3
+ * inputs); psi_i may be NULL at the REAL level.  The forward transform is a
+ * float32 cuFFT R2C, the -1/k^2 divide and the inverse are float64 (as NumPy
+ * evaluates them), so chi agrees with the reference to a float32 ulp or two.
+ * cuFFT plans and scratch live in ctx.
+ * ------------------------------------------------------------------------ */
+int lfm_poisson_chi_f32(lfm_context* ctx, int level, const float* psi_r, const float* psi_i,
+                        int N, double chi0, double kappa, double e0_sq,
+                        double boundary_fraction, int frozen, float* chi_out, void* stream);
+
 /* Out-of-place form of lfm_leapfrog_real_f32 / lfm_leapfrog_complex_f32
  * (level LFM_REAL or LFM_COMPLEX): the same step and the same bits, with the
  * new fields written to *_out instead of over the previous ones, which stay

@@ -150,10 +150,21 @@ struct FftSlot {
   float* sa_raw = nullptr;  // 3 * N^3, for protocol colour steps
 };
 
+// Poisson equilibration scratch per lattice edge: float32 R2C of the
+// right-hand side, float64 Z2D of the divided spectrum.
+struct PoissonSlot {
+  cufftHandle r2c = 0, z2d = 0;
+  float* rhs = nullptr;       // N^3
+  float2* spec_f = nullptr;   // N * N * (N/2+1)
+  double2* spec_d = nullptr;  // N * N * (N/2+1)
+  double* out = nullptr;      // N^3
+};
+
 struct lfm_context {
   int device = 0;
   std::mutex mu;
   std::map<int, FftSlot> slots;
+  std::map<int, PoissonSlot> poisson;
   double* metric_partials = nullptr;  // kMetricRows x kPartialStride, then the final row
 };
 
@@ -182,6 +193,30 @@ int fft_slot(lfm_context* ctx, int N, bool need_sa_raw, FftSlot** out) {
   if (need_sa_raw && !s.sa_raw) {
     e = cudaMalloc(&s.sa_raw, sizeof(float) * 3 * (size_t)N * N * N);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc S_a scratch");
+  }
+  *out = &s;
+  return LFM_OK;
+}
+
+int poisson_slot(lfm_context* ctx, int N, PoissonSlot** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != ctx->device)
+    return fail(LFM_ERR_INVALID_ARG, "context belongs to device %d, current device is %d",
+                ctx->device, dev);
+  PoissonSlot& s = ctx->poisson[N];
+  if (!s.out) {
+    const size_t n3 = (size_t)N * N * N, nc = (size_t)N * N * (N / 2 + 1);
+    if (cufftPlan3d(&s.r2c, N, N, N, CUFFT_R2C) != CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlan3d R2C N=%d", N);
+    if (cufftPlan3d(&s.z2d, N, N, N, CUFFT_Z2D) != CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlan3d Z2D N=%d", N);
+    e = cudaMalloc(&s.rhs, sizeof(float) * n3);
+    if (e == cudaSuccess) e = cudaMalloc(&s.spec_f, sizeof(float2) * nc);
+    if (e == cudaSuccess) e = cudaMalloc(&s.spec_d, sizeof(double2) * nc);
+    if (e == cudaSuccess) e = cudaMalloc(&s.out, sizeof(double) * n3);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc Poisson scratch");
   }
   *out = &s;
   return LFM_OK;
@@ -432,6 +467,15 @@ int lfm_context_destroy(lfm_context* ctx) {
     if (kv.second.spec) cudaFree(kv.second.spec);
     if (kv.second.sa_raw) cudaFree(kv.second.sa_raw);
   }
+  for (auto& kv : ctx->poisson) {
+    PoissonSlot& p = kv.second;
+    if (p.r2c) cufftDestroy(p.r2c);
+    if (p.z2d) cufftDestroy(p.z2d);
+    if (p.rhs) cudaFree(p.rhs);
+    if (p.spec_f) cudaFree(p.spec_f);
+    if (p.spec_d) cudaFree(p.spec_d);
+    if (p.out) cudaFree(p.out);
+  }
   if (ctx->metric_partials) cudaFree(ctx->metric_partials);
   cudaSetDevice(prev);
   delete ctx;
@@ -486,6 +530,44 @@ int lfm_leapfrog_complex_f32(const float* psi_r, float* psi_r_prev_io, const flo
   a.lut = device_lut(mask_table, lut);
   a.damp_prev = damp_prev ? 1 : 0;
   return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_poisson_chi_f32(lfm_context* ctx, int level, const float* psi_r, const float* psi_i,
+                        int N, double chi0, double kappa, double e0_sq,
+                        double boundary_fraction, int frozen, float* chi_out, void* stream) {
+  if (!ctx) return fail(LFM_ERR_INVALID_ARG, "null context");
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (level < LFM_REAL || level > LFM_COLOR) return fail(LFM_ERR_INVALID_ARG, "level %d", level);
+  if (!psi_r || !chi_out || (level != LFM_REAL && !psi_i))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  if (frozen && !(boundary_fraction > 0.0 && boundary_fraction < 1.0))
+    return fail(LFM_ERR_INVALID_ARG, "boundary_fraction %g", boundary_fraction);
+  const int colours = level == LFM_COLOR ? 3 : 1;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r, colours * b}, {psi_i, psi_i ? colours * b : 0}}, {{chi_out, b}});
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  PoissonSlot* s = nullptr;
+  rc = poisson_slot(ctx, N, &s);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = lfm::launch_poisson_rhs(psi_r, level == LFM_REAL ? nullptr : psi_i, s->rhs, N,
+                                          colours, (float)kappa, (float)e0_sq, st);
+  if (e != cudaSuccess) return cuda_fail(e, "Poisson rhs launch");
+  if (cufftSetStream(s->r2c, st) != CUFFT_SUCCESS ||
+      cufftExecR2C(s->r2c, s->rhs, reinterpret_cast<cufftComplex*>(s->spec_f)) != CUFFT_SUCCESS)
+    return fail(LFM_ERR_CUFFT, "cufftExecR2C N=%d", N);
+  e = lfm::launch_poisson_divide(s->spec_f, s->spec_d, N, st);
+  if (e != cudaSuccess) return cuda_fail(e, "Poisson divide launch");
+  if (cufftSetStream(s->z2d, st) != CUFFT_SUCCESS ||
+      cufftExecZ2D(s->z2d, reinterpret_cast<cufftDoubleComplex*>(s->spec_d), s->out) !=
+          CUFFT_SUCCESS)
+    return fail(LFM_ERR_CUFFT, "cufftExecZ2D N=%d", N);
+  e = lfm::launch_poisson_finish(s->out, chi_out, N, (float)chi0,
+                                 N / 2.0 * (1.0 - boundary_fraction), frozen ? 1 : 0, st);
+  if (e != cudaSuccess) return cuda_fail(e, "Poisson finish launch");
+  return LFM_OK;
 }
 
 int lfm_advance_f32(int level, const float* psi_r, const float* psi_r_prev, float* psi_r_out,

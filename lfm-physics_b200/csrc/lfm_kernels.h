@@ -50,6 +50,13 @@ cudaError_t launch_helmholtz_multiply_gd(float2* spec, int N, double gamma, doub
                                          cudaStream_t stream);
 cudaError_t launch_clip(const float* in, float* out, int64_t count, cudaStream_t stream);
 
+// Poisson equilibration pieces (poisson.cu).
+cudaError_t launch_poisson_rhs(const float* pr, const float* pi, float* rhs, int N, int colours,
+                               float kappa, float e0_sq, cudaStream_t stream);
+cudaError_t launch_poisson_divide(const float2* in, double2* out, int N, cudaStream_t stream);
+cudaError_t launch_poisson_finish(const double* dchi, float* chi, int N, float chi0,
+                                  double radius, int frozen, cudaStream_t stream);
+
 // Adjoint step (adjoint.cu).  g_out / g_in: adjoints of (psi_r, psi_r_prev,
 // psi_i, psi_i_prev, chi, chi_prev) after / before the step.
 cudaError_t launch_adjoint_step(int level, int N, const float* pr, const float* pi,

@@ -15,6 +15,9 @@ Contents
   the reference ``Backend`` signatures (lfm/core/backends/protocol.py:65-136),
   computed by the C restatement in ``lfm_oracle.cpp`` (float32: bit-exact to
   NumPy's float32 path; float64: the FP64 oracle).
+* ``gaussian_soliton`` / ``equilibrate_chi`` / ``interior_mask`` -- the
+  packet builder and the Poisson equilibration of lfm/fields/soliton.py and
+  lfm/fields/equilibrium.py (NumPy restatements).
 * seeded initial-condition builders for the benchmark and parity workloads.
 
 Parity pins: ``tests/golden/`` holds fixtures produced by the reference
@@ -121,6 +124,60 @@ def helmholtz_sa(color_energy: np.ndarray, N: int, sa_gamma: float, sa_d: float)
         s3 = np.fft.irfftn(h * hat, s=(N, N, N), axes=(0, 1, 2))
         out[a] = np.clip(s3, 0.0, None).astype(out_dtype).ravel()
     return out
+
+
+def gaussian_soliton(N: int, position, amplitude: float, sigma: float, phase: float = 0.0):
+    """Gaussian packet as lfm/fields/soliton.py:49-59 evaluates it: float32
+    grid, float32 r^2 and envelope, times cos / sin of the phase."""
+    x = np.arange(N, dtype=np.float32)
+    px, py, pz = position
+    r2 = ((x - px) ** 2)[:, None, None] + ((x - py) ** 2)[None, :, None] \
+        + ((x - pz) ** 2)[None, None, :]
+    env = amplitude * np.exp(-r2 / (2.0 * sigma**2))
+    return (env * np.cos(phase)).astype(np.float32), (env * np.sin(phase)).astype(np.float32)
+
+
+def interior_mask(N: int, boundary_fraction: float) -> np.ndarray:
+    """lfm/analysis/structure.py:148-171: dist <= N/2 (1 - bf), float64 distances."""
+    c = N / 2.0
+    x = np.arange(N, dtype=np.float64)
+    d2 = ((x - c) ** 2)[:, None, None] + ((x - c) ** 2)[None, :, None] \
+        + ((x - c) ** 2)[None, None, :]
+    return np.sqrt(d2) <= c * (1.0 - boundary_fraction)
+
+
+def equilibrate_chi(psi_r: np.ndarray, psi_i, chi0: float, kappa: float, e0_sq: float = 0.0,
+                    boundary_fraction: float | None = None) -> np.ndarray:
+    """Poisson-equilibrated chi, restating lfm/fields/equilibrium.py:26-121.
+
+    |Psi|^2 in float32 (colour sums over axis 0), rhs = kappa (|Psi|^2 - e0^2)
+    in float32, a float32 forward FFT (NumPy >= 2 keeps single precision),
+    the -1/k^2 divide in float64 (DC set to 0), a float64 inverse, then
+    chi = chi0 + dchi in float32 and chi0 on the frozen shell
+    (~interior_mask) when boundary_fraction is given.
+    """
+    if psi_r.ndim == 3:
+        psi_sq = psi_r**2
+        if psi_i is not None:
+            psi_sq = psi_sq + psi_i**2
+    else:
+        psi_sq = np.sum(psi_r**2, axis=0)
+        if psi_i is not None:
+            psi_sq = psi_sq + np.sum(psi_i**2, axis=0)
+    N = psi_sq.shape[0]
+    rhs = kappa * (psi_sq - e0_sq)
+    src = np.fft.rfftn(rhs)
+    k = np.fft.fftfreq(N) * 2.0 * np.pi
+    kz = np.fft.rfftfreq(N) * 2.0 * np.pi
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    k2[0, 0, 0] = 1.0
+    phi = -src / k2
+    phi[0, 0, 0] = 0.0
+    dchi = np.fft.irfftn(phi, s=(N, N, N), axes=(0, 1, 2)).astype(np.float32)
+    chi = (chi0 + dchi).astype(np.float32)
+    if boundary_fraction is not None:
+        chi[~interior_mask(N, boundary_fraction)] = chi0
+    return chi
 
 
 def color_energy(psi_r: np.ndarray, psi_i: np.ndarray, N: int) -> np.ndarray:

@@ -7,8 +7,9 @@ Run in a checkout that has the reference package importable, e.g.::
 Every array here comes from the reference's own code: ``NumpyBackend``
 (lfm/core/backends/numpy_backend.py), ``laplacian_19pt``
 (lfm/core/stencils.py), ``Evolver`` (lfm/core/evolver.py),
-``compute_metrics`` / ``interior_mask`` (lfm/analysis/) and
-``gaussian_soliton`` (lfm/fields/soliton.py).  The tests compare the oracle
+``compute_metrics`` / ``interior_mask`` (lfm/analysis/), ``gaussian_soliton``
+(lfm/fields/soliton.py), ``equilibrate_from_fields``
+(lfm/fields/equilibrium.py) and ``sweep`` / ``sweep_2d`` (lfm/sweep.py).  The tests compare the oracle
 and the CUDA path with these files; the reference is never needed at test
 time.
 """
@@ -198,6 +199,47 @@ def metrics_fixture() -> None:
                         real=np.array(json.dumps(m_real)), complex=np.array(json.dumps(m_cplx)))
 
 
+def equilibrium_fixture() -> None:
+    """gaussian_soliton and the Poisson equilibration (lfm/fields/equilibrium.py)."""
+    from lfm.fields.equilibrium import equilibrate_from_fields
+
+    data = {}
+    for N, bf in ((16, 0.3), (20, 0.15), (24, 0.3)):
+        pr1, pi1 = gaussian_soliton(N, (N / 2, N / 2 - 2.5, N / 2 + 1.0), 5.0, 2.0, 0.7)
+        pr2, pi2 = gaussian_soliton(N, (N / 2 - 3.0, N / 2 + 3.0, N / 2), 3.0, 1.5, 2.0)
+        pr, pi = (pr1 + pr2).astype(np.float32), (pi1 + pi2).astype(np.float32)
+        bmask = ~interior_mask(N, bf)
+        data[f"pr_{N}"], data[f"pi_{N}"] = pr, pi
+        data[f"soliton1_{N}"] = pr1
+        data[f"chi_real_{N}"] = equilibrate_from_fields(pr, None, CHI0, KAPPA, 0.0, bmask)
+        data[f"chi_complex_{N}"] = equilibrate_from_fields(pr, pi, CHI0, KAPPA, 0.0, bmask)
+        data[f"chi_free_{N}"] = equilibrate_from_fields(pr, pi, CHI0, 2 * KAPPA, 0.5, None)
+        col_r = np.stack([pr, 0.5 * pr, pi]).astype(np.float32)
+        col_i = np.stack([pi, pr, 0.25 * pi]).astype(np.float32)
+        data[f"colr_{N}"], data[f"coli_{N}"] = col_r, col_i
+        data[f"chi_color_{N}"] = equilibrate_from_fields(col_r, col_i, CHI0, KAPPA, 0.0, bmask)
+        data[f"bf_{N}"] = np.float64(bf)
+    np.savez_compressed(OUT / "equilibrium.npz", **data)
+
+
+def sweep_fixture() -> None:
+    """lfm.sweep on small lattices (Simulation on the NumPy backend)."""
+    from lfm.config_presets import gravity_em
+    from lfm.sweep import sweep, sweep_2d
+
+    runs = {
+        "kappa_real": sweep(gravity_only(16), "kappa", [1.0 / 63.0, 2.0 / 63.0], 12,
+                            soliton={"amplitude": 4.0, "sigma": 2.0}),
+        "grid_complex": sweep(gravity_em(16), "grid_size", [16, 20], 10,
+                              soliton={"amplitude": 3.0, "sigma": 2.0, "phase": 0.5}),
+        "plain_noeq": sweep(gravity_only(16), "chi0", [19.0, 18.0], 6, equilibrate=False),
+        "two_d": sweep_2d(gravity_em(12), "kappa", [1.0 / 63.0, 3.0 / 63.0], "epsilon_w",
+                          [0.1, 0.2], 8, metric_names=["chi_min", "energy_total"],
+                          soliton={"amplitude": 2.0, "sigma": 1.5}),
+    }
+    np.savez_compressed(OUT / "sweep.npz", runs=np.array(json.dumps(runs)))
+
+
 if __name__ == "__main__":
     masks()
     stencil()
@@ -205,4 +247,6 @@ if __name__ == "__main__":
     parity_runs()
     metrics_fixture()
     config1()
+    equilibrium_fixture()
+    sweep_fixture()
     print("fixtures written to", OUT)
