@@ -56,6 +56,10 @@ def parse():
     ap.add_argument("--batch-lattices", type=int, default=256)
     ap.add_argument("--batch-steps", type=int, default=200)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--level", choices=["real", "complex"], default="real",
+                    help="level of the main leg; complex (with the packets as both parts) is a "
+                         "secondary workload and turns the e2e, compensated and CPU legs off")
+    ap.add_argument("--batch-tuning", choices=["auto", "default"], default="auto")
     ap.add_argument("--adjoint-steps", type=int, default=500)
     return ap.parse_args()
 
@@ -78,14 +82,14 @@ def measured_peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(N: int):
+def profiled_traffic(N: int, level: str = "real"):
     """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     try:
         d = json.loads(p.read_text())
-        e = d.get(f"real_{N}")
+        e = d.get(f"{level}_{N}")
         return None if e is None else float(e["dram_bytes_per_launch"])
     except Exception:  # noqa: BLE001
         return None
@@ -280,8 +284,10 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
 
     os.environ.setdefault("LFM_B200_TUNE_CACHE", str(Path(tempfile.gettempdir()) /
                                                      "lfm_b200_bench_tune.json"))
-    B = BatchedLattices(cfgs, backend=be, tuning="auto")
-    tune = B.tune_report
+    B = BatchedLattices(cfgs, backend=be,
+                        tuning="auto" if args.batch_tuning == "auto" else None)
+    tune = B.tune_report or {"best": dict(threads=256, stages=3, item_cells=65536),
+                             "ms_per_step": None, "trials": []}
     B.graph_block = steps
     for i, (c, pr, pi) in enumerate(L):
         load(B, i, pr, pi)
@@ -429,8 +435,18 @@ def run_b200(args):
     N = args.N
     E, chi = real_solitons(N, seed_chi=1 + 1000 * rank, seed_solitons=2 + 1000 * rank)
     be = B200Backend(dev)
-    ev = Evolver(gravity_only(N), backend=be)
+    complex_level = args.level == "complex"
+    if complex_level:
+        from lfm_b200.config import gravity_em
+
+        args.no_e2e = args.no_compensated = args.no_cpu_baseline = True
+        main_cfg = gravity_em(N)
+    else:
+        main_cfg = gravity_only(N)
+    ev = Evolver(main_cfg, backend=be)
     ev.set_psi_real(E)
+    if complex_level:
+        ev.set_psi_imag(0.5 * E)
     ev.set_chi(chi)
     ev.evolve(max(args.warmup, 3))
     ev.warm_graphs()
@@ -468,10 +484,11 @@ def run_b200(args):
     cells = N**3
     value = world * cells * args.steps / (ms / 1e3) / 1e9
     ms_per_step = ms / args.steps
-    cfg_used = _lib.tune_get(0, N)
+    cfg_used = _lib.tune_get(int(main_cfg.field_level), N)
 
     peak, peak_kind = measured_peaks()
-    bytes_per_launch = BYTES_PER_CELL["real"] * cells
+    bpc = 36 if complex_level else BYTES_PER_CELL["real"]
+    bytes_per_launch = bpc * cells
     achieved = bytes_per_launch / (ms_per_step / 1e3) / 1e9
 
     # ---- compensated float32 variant (Delta form, 32 B/cell) ---------------
@@ -552,14 +569,17 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"REAL {N}^3 leapfrog step (GOV-01 + GOV-02, 19-point, sponge), "
-                               "64 packets, chi0 = 19 +- 1e-3",
-                   "N": N, "level": "REAL", "buffers": "resident", "bytes_per_cell": 24,
-                   "l2": "inputs 2.1 GB > L2, no flush", "parallelism": f"independent lattices x{world}",
-                   "tile": cfg_used},
+        "config": {"workload": f"{args.level.upper()} {N}^3 leapfrog step (GOV-01 + GOV-02, "
+                               "19-point, sponge), 64 packets, chi0 = 19 +- 1e-3",
+                   "N": N, "level": args.level.upper(), "buffers": "resident",
+                   "bytes_per_cell": bpc,
+                   "l2": f"inputs {4 * bpc // 6 * cells / 1e9:.2f} GB"
+                         + (" > L2, no flush" if 4 * bpc // 6 * cells > 126e6 else
+                            " (within L2: profiling size only)"),
+                   "parallelism": f"independent lattices x{world}", "tile": cfg_used},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": profiled_traffic(N),
+                     "traffic": profiled_traffic(N, args.level),
                      "algorithmic_bytes_per_launch": bytes_per_launch},
         "clocks": clock_info,
         "gpu_launches": args.steps,
