@@ -581,6 +581,24 @@ struct QFields {
   static constexpr int ns = (LEVEL == LFM_REAL) ? 2 : 3;
 };
 
+// Tile geometry of a march.  GeomRT reads it from the parameters (any
+// lattice, any tile); GeomCT<N, TJ, NS> fixes it at compile time for the
+// headline tiles (3 stages, resident point fields), so every shared-memory
+// offset of a plane folds into an immediate beside one per-thread base.
+struct GeomRT {
+  static constexpr bool kFixed = false;
+  int N, TJ, S, SF;
+  __device__ __forceinline__ explicit GeomRT(const TmaParams& P)
+      : N(P.N), TJ(P.TJ), S(P.S), SF(P.stage_floats) {}
+};
+
+template <int N_, int TJ_, int NS_>
+struct GeomCT {
+  static constexpr bool kFixed = true;
+  static constexpr int N = N_, TJ = TJ_, S = 3, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
+  __device__ __forceinline__ explicit GeomCT(const TmaParams&) {}
+};
+
 // Shared bookkeeping of the barrier-free march.
 struct QShared {
   uint32_t done[kMaxStages];  // warps finished with the stage's current plane
@@ -593,21 +611,27 @@ struct QShared {
 // the centre plane's stage when it is done with it, and the last warp to do
 // so refills the stage with the plane S further on.  Returns false when the
 // CTA must stop (a bounded wait gave up).
-template <int LEVEL, int V, bool COMP, bool PARTIAL, int PA, int PB, int PC>
+// SCUR / SNXT: the stages of the centre and the next plane when the
+// geometry fixes them (3 stages, the loop unrolled by 3), else -1.
+template <int LEVEL, int V, bool COMP, bool PARTIAL, int PA, int PB, int PC, class G = GeomRT,
+          int SCUR = -1, int SNXT = -1>
 __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
                                         const QLane& L, int c, int i0, int i1, int j0,
-                                        int nplanes, int nwarps, int& s_cur, int& s_nxt,
+                                        int nplanes, int nwarps, int& s_cur_rt, int& s_nxt_rt,
                                         uint32_t& ph_nxt, const QKeys<V>& K,
                                         bool lane_active) {
   // PARTIAL: the CTA may be wider than the tile (batch kernel)
   const bool active = !PARTIAL || lane_active;
   constexpr int NS = QFields<LEVEL>::ns;
   const StepArgs& a = P.a;
-  const int N = P.N, TJ = P.TJ;
+  const G g(P);
+  const int N = g.N, TJ = g.TJ;
   const int FB = (TJ + 2) * N;
   const int PTS = TJ * N;  // point-field stride
-  const int SF = P.stage_floats;
+  const int SF = g.SF;
+  const int s_cur = SCUR >= 0 ? SCUR : s_cur_rt;
+  const int s_nxt = SNXT >= 0 ? SNXT : s_nxt_rt;
   if (*(volatile int*)&sh.abort_flag) return false;
   if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
     *(volatile int*)&sh.abort_flag = 1;
@@ -734,20 +758,25 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     }
   }
   __syncwarp();
-  s_cur = s_nxt;
-  s_nxt = (s_nxt + 1 == P.S) ? 0 : s_nxt + 1;
-  if (s_nxt == 0) ph_nxt ^= 1u;
+  if constexpr (SNXT >= 0) {
+    if (SNXT == 2) ph_nxt ^= 1u;  // the next plane's stage wraps to 0
+  } else {
+    s_cur_rt = s_nxt_rt;
+    s_nxt_rt = (s_nxt_rt + 1 == P.S) ? 0 : s_nxt_rt + 1;
+    if (s_nxt_rt == 0) ph_nxt ^= 1u;
+  }
   return true;
 }
 
 // The march of one tile: rows j0 .. j0+rows-1 (all k), planes [i0, i1).
 // Initialises the stage barriers and the bookkeeping itself, so a CTA may
 // run several marches one after another (the batch kernel).
-template <int LEVEL, int V, bool COMP, bool PARTIAL>
+template <int LEVEL, int V, bool COMP, bool PARTIAL, class G = GeomRT>
 __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, int j0, int i0, int i1, int rows) {
   constexpr int NS = QFields<LEVEL>::ns;
-  const int N = P.N, TJ = P.TJ, S = P.S;
+  const G g(P);
+  const int N = g.N, TJ = g.TJ, S = g.S;
   const int n = i1 - i0;
   const int nplanes = n + 2;
   const int tid = threadIdx.x;
@@ -802,8 +831,8 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   } else if (active) {
 #pragma unroll
     for (int f = 0; f < NS; ++f) {
-      q_load<V>(Q[f][0], smem, 0 * P.stage_floats + f * (TJ + 2) * N, L);
-      q_load<V>(Q[f][1], smem, (1 % S) * P.stage_floats + f * (TJ + 2) * N, L);
+      q_load<V>(Q[f][0], smem, 0 * g.SF + f * (TJ + 2) * N, L);
+      q_load<V>(Q[f][1], smem, (1 % S) * g.SF + f * (TJ + 2) * N, L);
     }
   }
   __syncthreads();
@@ -817,18 +846,21 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     int s_cur = 1 % S, s_nxt = 2 % S;
     uint32_t ph_nxt = (uint32_t)((2 / S) & 1);
     int c = 0;
+    // With a fixed 3-stage geometry, unrolled position p of the loop always
+    // has its centre plane in stage (p + 1) % 3 and the next in (p + 2) % 3.
+    constexpr bool F = G::kFixed;
     while (true) {
-      if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
-                                                      nplanes, nwarps, s_cur, s_nxt, ph_nxt, K,
-                                                      active))
+      if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2, G, F ? 1 : -1, F ? 2 : -1>(
+                        P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
+                        ph_nxt, K, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
-                                                        nplanes, nwarps, s_cur, s_nxt, ph_nxt,
-                                                        K, active))
+      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0, G, F ? 2 : -1, F ? 0 : -1>(
+                          P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
+                          ph_nxt, K, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1>(P, smem, bars, sh, Q, L, c, i0, i1, j0,
-                                                        nplanes, nwarps, s_cur, s_nxt, ph_nxt,
-                                                        K, active))
+      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1, G, F ? 0 : -1, F ? 1 : -1>(
+                          P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
+                          ph_nxt, K, active))
         break;
       ++c;
     }
@@ -842,14 +874,15 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   }
 }
 
-template <int LEVEL, int V, bool COMP>
+template <int LEVEL, int V, bool COMP, class G = GeomRT>
 __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
   __shared__ QShared sh;
+  const G g(P);
   const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
   const int i0 = ch * P.IC;
-  q_march<LEVEL, V, COMP, false>(P, smem, bars, sh, jt * P.TJ, i0, min(i0 + P.IC, P.N), P.TJ);
+  q_march<LEVEL, V, COMP, false, G>(P, smem, bars, sh, jt * g.TJ, i0, min(i0 + P.IC, g.N), g.TJ);
 }
 
 // ---- batch kernel: many lattices, one launch per step -------------------------
@@ -1098,6 +1131,57 @@ std::mutex KernelSlot<LEVEL, V, QUEUE, COMP>::mu;
 template <int LEVEL, int V, bool QUEUE, bool COMP>
 int KernelSlot<LEVEL, V, QUEUE, COMP>::granted = 0;
 
+// Compile-time tiles for the headline sizes (resident layout, 3 stages).
+template <int LEVEL, int V, int N, int TJ>
+struct FixedSlot {
+  static std::mutex mu;
+  static int granted;
+  static auto fn() { return tma_queue_kernel<LEVEL, V, false, GeomCT<N, TJ, QFields<LEVEL>::ns>>; }
+};
+template <int LEVEL, int V, int N, int TJ>
+std::mutex FixedSlot<LEVEL, V, N, TJ>::mu;
+template <int LEVEL, int V, int N, int TJ>
+int FixedSlot<LEVEL, V, N, TJ>::granted = 0;
+
+struct FixedTile {
+  int level, V, N, TJ;
+};
+constexpr FixedTile kFixedTiles[] = {
+    {LFM_REAL, 4, 512, 4}, {LFM_REAL, 4, 256, 8}, {LFM_COMPLEX, 2, 512, 2},
+    {LFM_COMPLEX, 2, 256, 4}, {LFM_REAL, 4, 128, 8}, {LFM_COMPLEX, 2, 128, 4}};
+
+// The fixed tile for (level, V, N), if any.
+const FixedTile* fixed_tile(int level, int V, int N) {
+  for (const FixedTile& t : kFixedTiles)
+    if (t.level == level && t.V == V && t.N == N) return &t;
+  return nullptr;
+}
+
+template <int LEVEL, int V, int N, int TJ>
+cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
+  using Slot = FixedSlot<LEVEL, V, N, TJ>;
+  return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
+}
+
+// Launches the compile-time variant when the chosen tile is one of
+// kFixedTiles (3 stages, no streamed mask or S_a); false if there is none.
+template <int LEVEL, int V>
+bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
+  if (ch.S != 3 || P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0) return false;
+  const FixedTile* t = fixed_tile(LEVEL, V, P.N);
+  if (!t || t->TJ != ch.TJ) return false;
+  if constexpr (LEVEL == LFM_REAL && V == 4) {
+    if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 4>(P, ch, stream); return true; }
+    if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 8>(P, ch, stream); return true; }
+    if (P.N == 128) { *err = launch_fixed<LEVEL, V, 128, 8>(P, ch, stream); return true; }
+  } else if constexpr (LEVEL == LFM_COMPLEX && V == 2) {
+    if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 2>(P, ch, stream); return true; }
+    if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 4>(P, ch, stream); return true; }
+    if (P.N == 128) { *err = launch_fixed<LEVEL, V, 128, 4>(P, ch, stream); return true; }
+  }
+  return false;
+}
+
 template <int LEVEL, int V, bool QUEUE, bool COMP = false>
 cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t stream) {
   using Slot = KernelSlot<LEVEL, V, QUEUE, COMP>;
@@ -1111,6 +1195,15 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // instead is slower, bank conflicts of the random-key loads).
   const int count = (P.pf_mask >= 0) ? 0 : P.a.lut.count;
   const int table_bytes = 4 * count;
+  // Without a forced tile, the sizes with a compile-time variant take its
+  // tile (TJ rows, 3 stages); the planner still picks the plane chunk.
+  TileConfig fixed_cfg;
+  const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns)
+                            ? fixed_tile(LEVEL, V, P.N) : nullptr;
+  if (!forced && ft) {
+    fixed_cfg = TileConfig{ft->TJ, 3, 0, 0, 0, V};
+    forced = &fixed_cfg;
+  }
   const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0,
                            table_bytes);
   if (!ch.TJ) return cudaErrorNotSupported;
@@ -1121,6 +1214,10 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   P.stage_floats = stage_bytes(P.N, ch.TJ, P.ns, P.np) / 4;
   TileConfig used{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem, V};
   tune_record(LEVEL, P.N, used);
+  if constexpr (QUEUE && !COMP) {
+    cudaError_t fe = cudaSuccess;
+    if (try_fixed<LEVEL, V>(P, ch, stream, &fe)) return fe;
+  }
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
 
