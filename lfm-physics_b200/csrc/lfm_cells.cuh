@@ -11,21 +11,24 @@
 namespace lfm {
 
 // ---- REAL (numpy_backend.py:80-130) ---------------------------------------
-struct RealOut {
-  float psi, psi_prev, chi, chi_prev;
+// T = float for one cell, F2 for two cells packed (same operations per cell).
+template <class T>
+struct RealOutT {
+  T psi, psi_prev, chi, chi_prev;
 };
+using RealOut = RealOutT<float>;
 
-__device__ __forceinline__ RealOut real_cell(float lapE, float e, float e_prev, float lapX,
-                                             float chi, float chi_prev, float mask,
-                                             const StepConsts& s) {
-  const float chi_sq = fmul(chi, chi);
-  const float E_new = gov01(e, e_prev, lapE, chi_sq, s);
+template <class T>
+__device__ __forceinline__ RealOutT<T> real_cell(T lapE, T e, T e_prev, T lapX, T chi,
+                                                 T chi_prev, T mask, const StepConsts& s) {
+  const T chi_sq = fmul(chi, chi);
+  const T E_new = gov01(e, e_prev, lapE, chi_sq, s);
   // chi_source = (kappa/chi0)*chi*(E*E - e0_sq)
-  const float src = fmul(fmul(s.k_over_chi0, chi), fsub(fmul(e, e), s.e0_sq));
-  float acc = fsub(lapX, src);
+  const T src = fmul(fmul(cst<T>(s.k_over_chi0), chi), fsub(fmul(e, e), cst<T>(s.e0_sq)));
+  T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
-  const float absorb = fsub(1.0f, mask);
-  RealOut o;
+  const T absorb = fsub(cst<T>(1.0f), mask);
+  RealOutT<T> o;
   o.psi = fmul(E_new, absorb);
   o.psi_prev = fmul(e, absorb);
   o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
@@ -34,40 +37,54 @@ __device__ __forceinline__ RealOut real_cell(float lapE, float e, float e_prev, 
 }
 
 // ---- COMPLEX (numpy_backend.py:132-205) -----------------------------------
-struct ComplexOut {
-  float pr, pr_prev, pi, pi_prev, chi, chi_prev;
+template <class T>
+struct ComplexOutT {
+  T pr, pr_prev, pi, pi_prev, chi, chi_prev;
 };
+using ComplexOut = ComplexOutT<float>;
 
 // Face neighbours of one field, for the momentum current.
-struct Faces {
-  float im, ip, jm, jp, km, kp;
+template <class T>
+struct FacesT {
+  T im, ip, jm, jp, km, kp;
 };
+using Faces = FacesT<float>;
 
-__device__ __forceinline__ float momentum_current(float pr, float pi, const Faces& R,
-                                                  const Faces& I) {
-  const float jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
-  const float jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
-  const float jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
-  return fmul(0.5f, fadd(fadd(jx, jy), jz));  // j_total = 0.5*(j_x + j_y + j_z)
+__device__ __forceinline__ FacesT<F2> pk_faces(const Faces& a, const Faces& b) {
+  FacesT<F2> f;
+  f.im = pk(a.im, b.im); f.ip = pk(a.ip, b.ip);
+  f.jm = pk(a.jm, b.jm); f.jp = pk(a.jp, b.jp);
+  f.km = pk(a.km, b.km); f.kp = pk(a.kp, b.kp);
+  return f;
 }
 
-__device__ __forceinline__ ComplexOut complex_cell(float lapR, float pr, float pr_prev,
-                                                   const Faces& R, float lapI, float pi,
-                                                   float pi_prev, const Faces& I, float lapX,
-                                                   float chi, float chi_prev, float mask,
-                                                   const StepConsts& s) {
-  const float chi_sq = fmul(chi, chi);
-  const float Pr_new = gov01(pr, pr_prev, lapR, chi_sq, s);
-  const float Pi_new = gov01(pi, pi_prev, lapI, chi_sq, s);
-  const float psi_sq = fadd(fmul(pr, pr), fmul(pi, pi));
-  const float jt = momentum_current(pr, pi, R, I);
+template <class T>
+__device__ __forceinline__ T momentum_current(T pr, T pi, const FacesT<T>& R,
+                                              const FacesT<T>& I) {
+  const T jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
+  const T jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
+  const T jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
+  return fmul(cst<T>(0.5f), fadd(fadd(jx, jy), jz));  // j_total = 0.5*(j_x + j_y + j_z)
+}
+
+template <class T>
+__device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
+                                                       const FacesT<T>& R, T lapI, T pi,
+                                                       T pi_prev, const FacesT<T>& I, T lapX,
+                                                       T chi, T chi_prev, T mask,
+                                                       const StepConsts& s) {
+  const T chi_sq = fmul(chi, chi);
+  const T Pr_new = gov01(pr, pr_prev, lapR, chi_sq, s);
+  const T Pi_new = gov01(pi, pi_prev, lapI, chi_sq, s);
+  const T psi_sq = fadd(fmul(pr, pr), fmul(pi, pi));
+  const T jt = momentum_current(pr, pi, R, I);
   // (kappa/chi0)*chi*(psi_sq + eps_w*j - e0_sq)
-  const float src =
-      fmul(fmul(s.k_over_chi0, chi), fsub(fadd(psi_sq, fmul(s.eps_w, jt)), s.e0_sq));
-  float acc = fsub(lapX, src);
+  const T src = fmul(fmul(cst<T>(s.k_over_chi0), chi),
+                     fsub(fadd(psi_sq, fmul(cst<T>(s.eps_w), jt)), cst<T>(s.e0_sq)));
+  T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
-  const float absorb = fsub(1.0f, mask);
-  ComplexOut o;
+  const T absorb = fsub(cst<T>(1.0f), mask);
+  ComplexOutT<T> o;
   o.pr = fmul(Pr_new, absorb);
   o.pi = fmul(Pi_new, absorb);
   o.pr_prev = fmul(pr, absorb);

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "lfm_b200.h"
@@ -18,6 +19,39 @@ namespace lfm {
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+// Two cells' values in one 64-bit register pair, for Blackwell's packed
+// FADD2 / FMUL2: each lane is rounded on its own exactly as the scalar
+// operation rounds it, so a cell's bits do not depend on the packing.
+struct F2 {
+  float2 v;
+};
+__device__ __forceinline__ F2 pk(float a, float b) { return F2{make_float2(a, b)}; }
+__device__ __forceinline__ F2 fadd(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fmul(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fsub(F2 a, F2 b) {
+  unsigned long long ra, rb, rd;
+  memcpy(&ra, &a.v, 8);
+  memcpy(&rb, &b.v, 8);
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  F2 d;
+  memcpy(&d.v, &rd, 8);
+  return d;
+}
+
+// A float constant as the value type T (broadcast to both lanes for F2).
+template <class T>
+__device__ __forceinline__ T cst(float a);
+template <>
+__device__ __forceinline__ float cst<float>(float a) { return a; }
+template <>
+__device__ __forceinline__ F2 cst<F2>(float a) { return pk(a, a); }
+
+// x < lo ? lo : x per lane (a NaN stays NaN, as NumPy's boolean-mask clamp keeps it)
+__device__ __forceinline__ float clamp_below(float x, float lo) { return x < lo ? lo : x; }
+__device__ __forceinline__ F2 clamp_below(F2 x, float lo) {
+  return pk(x.v.x < lo ? lo : x.v.x, x.v.y < lo ? lo : x.v.y);
+}
 
 // Scalar parameters rounded to float32 on the host the way NumPy rounds a
 // Python float that meets a float32 array (NEP 50 "weak" scalars).  Compound
@@ -96,33 +130,66 @@ __device__ __forceinline__ float lap19(const S19& f) {
   return fadd(fadd(fmul(face_w, faces), fmul(edge_w, edges)), fmul(-4.0f, f.c));
 }
 
+// The pointwise helpers below take T = float (one cell) or F2 (two cells,
+// packed); both evaluate the same operations in the same order per cell.
+
 // GOV-01: 2.0*P - P_prev + dt2*(lap - chi_sq*P)   (numpy_backend.py:108)
-__device__ __forceinline__ float gov01(float p, float p_prev, float lap, float chi_sq,
-                                       const StepConsts& s) {
-  return fadd(fsub(fmul(2.0f, p), p_prev), fmul(s.dt2, fsub(lap, fmul(chi_sq, p))));
+template <class T>
+__device__ __forceinline__ T gov01(T p, T p_prev, T lap, T chi_sq, const StepConsts& s) {
+  return fadd(fsub(fmul(cst<T>(2.0f), p), p_prev), fmul(cst<T>(s.dt2), fsub(lap, fmul(chi_sq, p))));
 }
 
 // chi_accel -= 4*lambda*chi*(chi^2 - chi0^2) when lambda > 0 (numpy_backend.py:113-114)
-__device__ __forceinline__ float mexican_hat(float acc, float chi, float chi_sq,
-                                             const StepConsts& s) {
+template <class T>
+__device__ __forceinline__ T mexican_hat(T acc, T chi, T chi_sq, const StepConsts& s) {
   if (!s.use_lambda) return acc;
-  return fsub(acc, fmul(fmul(s.four_lambda, chi), fsub(chi_sq, s.chi0_sq)));
+  return fsub(acc, fmul(fmul(cst<T>(s.four_lambda), chi), fsub(chi_sq, cst<T>(s.chi0_sq))));
 }
 
 // 2.0*chi - chi_prev + dt2*accel, clamp at -chi0, sponge blend
 // mask*chi0 + (1-mask)*chi_new   (numpy_backend.py:115-124)
-__device__ __forceinline__ float gov02_finish(float chi, float chi_prev, float acc, float mask,
-                                              float absorb, const StepConsts& s) {
-  float chi_new = fadd(fsub(fmul(2.0f, chi), chi_prev), fmul(s.dt2, acc));
-  if (chi_new < s.neg_chi0) chi_new = s.neg_chi0;
-  return fadd(fmul(mask, s.chi0), fmul(absorb, chi_new));
+template <class T>
+__device__ __forceinline__ T gov02_finish(T chi, T chi_prev, T acc, T mask, T absorb,
+                                          const StepConsts& s) {
+  T chi_new = fadd(fsub(fmul(cst<T>(2.0f), chi), chi_prev), fmul(cst<T>(s.dt2), acc));
+  chi_new = clamp_below(chi_new, s.neg_chi0);
+  return fadd(fmul(mask, cst<T>(s.chi0)), fmul(absorb, chi_new));
 }
 
 // One axis of the momentum current: Pr*(Pi[+] - Pi[-]) - Pi*(Pr[+] - Pr[-])
 // (numpy_backend.py:174-182, with np.roll(-1) the + neighbour).
-__device__ __forceinline__ float current_axis(float pr, float pi, float pr_p, float pr_m,
-                                              float pi_p, float pi_m) {
+template <class T>
+__device__ __forceinline__ T current_axis(T pr, T pi, T pr_p, T pr_m, T pi_p, T pi_m) {
   return fsub(fmul(pr, fsub(pi_p, pi_m)), fmul(pi, fsub(pr_p, pr_m)));
+}
+
+// lap19 of two cells at once.  The neighbours in i and j sit at the same
+// vector position as the cells, so those sums run packed; the k-neighbours
+// (k-1, k+1) are the next cell over, so those adds run per lane.  The order
+// of every cell's additions is the one lap19 uses.
+__device__ __forceinline__ F2 lap19_pair(const S19& a, const S19& b) {
+  F2 faces = fadd(pk(a.im, b.im), pk(a.ip, b.ip));
+  faces = fadd(faces, pk(a.jm, b.jm));
+  faces = fadd(faces, pk(a.jp, b.jp));
+  float fa = fadd(faces.v.x, a.km), fb = fadd(faces.v.y, b.km);
+  fa = fadd(fa, a.kp);
+  fb = fadd(fb, b.kp);
+  F2 edges = fadd(pk(a.imjm, b.imjm), pk(a.imjp, b.imjp));
+  edges = fadd(edges, pk(a.ipjm, b.ipjm));
+  edges = fadd(edges, pk(a.ipjp, b.ipjp));
+  float ea = edges.v.x, eb = edges.v.y;
+  ea = fadd(ea, a.imkm); eb = fadd(eb, b.imkm);
+  ea = fadd(ea, a.imkp); eb = fadd(eb, b.imkp);
+  ea = fadd(ea, a.ipkm); eb = fadd(eb, b.ipkm);
+  ea = fadd(ea, a.ipkp); eb = fadd(eb, b.ipkp);
+  ea = fadd(ea, a.jmkm); eb = fadd(eb, b.jmkm);
+  ea = fadd(ea, a.jmkp); eb = fadd(eb, b.jmkp);
+  ea = fadd(ea, a.jpkm); eb = fadd(eb, b.jpkm);
+  ea = fadd(ea, a.jpkp); eb = fadd(eb, b.jpkp);
+  const float face_w = (float)(1.0 / 3.0);
+  const float edge_w = (float)(1.0 / 6.0);
+  return fadd(fadd(fmul(cst<F2>(face_w), pk(fa, fb)), fmul(cst<F2>(edge_w), pk(ea, eb))),
+              fmul(cst<F2>(-4.0f), pk(a.c, b.c)));
 }
 
 // Mask value from the radial lookup table (see lfm_mask_lut in lfm_b200.h).

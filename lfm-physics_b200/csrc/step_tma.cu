@@ -632,6 +632,8 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   const int SF = g.SF;
   const int s_cur = SCUR >= 0 ? SCUR : s_cur_rt;
   const int s_nxt = SNXT >= 0 ? SNXT : s_nxt_rt;
+  // packed two-cell arithmetic in the compile-time tiles (V even)
+  constexpr bool PK = G::kFixed && (V % 2 == 0);
   if (*(volatile int*)&sh.abort_flag) return false;
   if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
     *(volatile int*)&sh.abort_flag = 1;
@@ -706,6 +708,25 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     const Vec<V> ep = lds<V>(smem, bc + L.o_pt);
     const Vec<V> xp = lds<V>(smem, bc + L.o_pt + PTS);
     float o_psi[V], o_chi[V], o_pp[V], o_cp[V];
+    if constexpr (PK) {
+      // two cells per packed FADD2 / FMUL2
+#pragma unroll
+      for (int e = 0; e < V; e += 2) {
+        const S19 E0 = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 E1 = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e + 1);
+        const S19 X0 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const S19 X1 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e + 1);
+        F2 epv = pk(ep.v[e], ep.v[e + 1]);
+        if (a.damp_prev) epv = fmul(epv, pk(absorb[e], absorb[e + 1]));
+        const RealOutT<F2> o =
+            real_cell(lap19_pair(E0, E1), pk(E0.c, E1.c), epv, lap19_pair(X0, X1),
+                      pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]), pk(mask[e], mask[e + 1]), a.c);
+        o_psi[e] = o.psi.v.x; o_psi[e + 1] = o.psi.v.y;
+        o_chi[e] = o.chi.v.x; o_chi[e + 1] = o.chi.v.y;
+        o_pp[e] = o.psi_prev.v.x; o_pp[e + 1] = o.psi_prev.v.y;
+        o_cp[e] = o.chi_prev.v.x; o_cp[e + 1] = o.chi_prev.v.y;
+      }
+    } else {
 #pragma unroll
     for (int e = 0; e < V; ++e) {
       const S19 E = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
@@ -713,6 +734,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       const float epv = a.damp_prev ? fmul(ep.v[e], absorb[e]) : ep.v[e];
       const RealOut o = real_cell(lap19(E), E.c, epv, lap19(X), X.c, xp.v[e], mask[e], a.c);
       o_psi[e] = o.psi; o_chi[e] = o.chi; o_pp[e] = o.psi_prev; o_cp[e] = o.chi_prev;
+    }
     }
     stg<V>(a.pr_out + gofs, o_psi);
     stg<V>(a.chi_out + gofs, o_chi);
@@ -723,6 +745,34 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     const Vec<V> ip = lds<V>(smem, bc + L.o_pt + PTS);
     const Vec<V> xp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
     float o_r[V], o_i[V], o_c[V], o_rp[V], o_ip[V], o_cp[V];
+    if constexpr (PK) {
+#pragma unroll
+      for (int e = 0; e < V; e += 2) {
+        const S19 R0 = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 R1 = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e + 1);
+        const S19 I0 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const S19 I1 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e + 1);
+        const S19 X0 = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
+        const S19 X1 = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e + 1);
+        F2 rpv = pk(rp.v[e], rp.v[e + 1]), ipv = pk(ip.v[e], ip.v[e + 1]);
+        if (a.damp_prev) {
+          const F2 ab = pk(absorb[e], absorb[e + 1]);
+          rpv = fmul(rpv, ab);
+          ipv = fmul(ipv, ab);
+        }
+        const ComplexOutT<F2> o = complex_cell(
+            lap19_pair(R0, R1), pk(R0.c, R1.c), rpv, pk_faces(faces_of(R0), faces_of(R1)),
+            lap19_pair(I0, I1), pk(I0.c, I1.c), ipv, pk_faces(faces_of(I0), faces_of(I1)),
+            lap19_pair(X0, X1), pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]),
+            pk(mask[e], mask[e + 1]), a.c);
+        o_r[e] = o.pr.v.x; o_r[e + 1] = o.pr.v.y;
+        o_i[e] = o.pi.v.x; o_i[e + 1] = o.pi.v.y;
+        o_c[e] = o.chi.v.x; o_c[e + 1] = o.chi.v.y;
+        o_rp[e] = o.pr_prev.v.x; o_rp[e + 1] = o.pr_prev.v.y;
+        o_ip[e] = o.pi_prev.v.x; o_ip[e + 1] = o.pi_prev.v.y;
+        o_cp[e] = o.chi_prev.v.x; o_cp[e + 1] = o.chi_prev.v.y;
+      }
+    } else {
 #pragma unroll
     for (int e = 0; e < V; ++e) {
       const S19 R = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
@@ -734,6 +784,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
                                         faces_of(I), lap19(X), X.c, xp.v[e], mask[e], a.c);
       o_r[e] = o.pr; o_i[e] = o.pi; o_c[e] = o.chi;
       o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev; o_cp[e] = o.chi_prev;
+    }
     }
     stg<V>(a.pr_out + gofs, o_r);
     stg<V>(a.pi_out + gofs, o_i);
