@@ -214,6 +214,20 @@ __device__ __forceinline__ float mask_from_q_flat(const MaskLut& m, int32_t q) {
   return in_band ? t : (q < m.q_lo ? 0.0f : 1.0f);
 }
 
+// mask_from_q_flat in two halves, so that a kernel can issue a cell's table
+// load one plane early and pick the value when it needs it:
+// mask_pick(m, q, mask_fetch(m, q)) == mask_from_q_flat(m, q).
+__device__ __forceinline__ float mask_fetch(const MaskLut& m, int32_t q) {
+  const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
+  float t = 0.0f;
+  if (in_band) t = __ldg(m.table + ((q - m.q_lo) >> m.shift));
+  return t;
+}
+__device__ __forceinline__ float mask_pick(const MaskLut& m, int32_t q, float t) {
+  const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
+  return in_band ? t : (q < m.q_lo ? 0.0f : 1.0f);
+}
+
 // Squared doubled offset from the lattice centre: (2x - N + 1)^2.
 __device__ __forceinline__ int32_t qterm(int x, int N) {
   const int32_t d = 2 * x - N + 1;

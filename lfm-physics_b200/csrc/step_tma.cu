@@ -620,7 +620,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
                                         const QLane& L, int c, int i0, int i1, int j0,
                                         int nplanes, int nwarps, int& s_cur_rt, int& s_nxt_rt,
                                         uint32_t& ph_nxt, const QKeys<V>& K,
-                                        bool lane_active) {
+                                        bool lane_active, float (&mraw)[V]) {
   // PARTIAL: the CTA may be wider than the tile (batch kernel)
   const bool active = !PARTIAL || lane_active;
   constexpr int NS = QFields<LEVEL>::ns;
@@ -656,6 +656,17 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     const Vec<V> m = lds<V>(smem, bc + L.o_pt + P.pf_mask * PTS);
 #pragma unroll
     for (int e = 0; e < V; ++e) mask[e] = m.v[e];
+  } else if constexpr (G::kFixed) {
+    // table values of this plane were fetched one plane ago; fetch the next
+    // plane's now, so their latency overlaps this plane's arithmetic
+    const int32_t qij = qterm(i, N) + K.qj;
+#pragma unroll
+    for (int e = 0; e < V; ++e) mask[e] = mask_pick(a.lut, qij + K.qk[e], mraw[e]);
+    if (c + 1 < i1 - i0) {
+      const int32_t qn = qterm(i + 1, N) + K.qj;
+#pragma unroll
+      for (int e = 0; e < V; ++e) mraw[e] = mask_fetch(a.lut, qn + K.qk[e]);
+    }
   } else {
     q_mask<V>(a.lut, qterm(i, N), K, mask);
   }
@@ -873,6 +884,16 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     sh.issued = first;
   }
   QPlane<V> Q[NS][3];
+  float mraw[V];  // sponge-table values fetched one plane ahead (fixed geometry)
+#pragma unroll
+  for (int e = 0; e < V; ++e) mraw[e] = 0.0f;
+  if constexpr (G::kFixed) {
+    if (P.pf_mask < 0 && active) {
+      const int32_t q0 = qterm(i0, N) + K.qj;
+#pragma unroll
+      for (int e = 0; e < V; ++e) mraw[e] = mask_fetch(P.a.lut, q0 + K.qk[e]);
+    }
+  }
   // planes i0-1 (u = 0, stage 0) and i0 (u = 1, stage 1): both first uses, parity 0
   bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitLimitNs);
   ok = mbar_wait_bounded(&bars[1 % S], 0u, kWaitLimitNs) && ok;
@@ -903,15 +924,15 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     while (true) {
       if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2, G, F ? 1 : -1, F ? 2 : -1>(
                         P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                        ph_nxt, K, active))
+                        ph_nxt, K, active, mraw))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0, G, F ? 2 : -1, F ? 0 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                          ph_nxt, K, active))
+                          ph_nxt, K, active, mraw))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1, G, F ? 0 : -1, F ? 1 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                          ph_nxt, K, active))
+                          ph_nxt, K, active, mraw))
         break;
       ++c;
     }
