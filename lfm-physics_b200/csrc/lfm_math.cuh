@@ -20,15 +20,21 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 
-// Two cells' values in one 64-bit register pair, for Blackwell's packed
-// FADD2 / FMUL2: each lane is rounded on its own exactly as the scalar
-// operation rounds it, so a cell's bits do not depend on the packing.
+// Two cells' values in one 64-bit register pair.  Additions and
+// subtractions run as Blackwell's packed FADD2 (each lane rounded on its own,
+// exactly as the scalar operation rounds it).  Multiplications stay two scalar
+// __fmul_rn: a packed FMUL2 feeding a packed FADD2 was measured to come out
+// fused (one rounding, about half of all results an ulp off), written with
+// the __fmul2_rn intrinsic (also under -fmad=false) or as mul.rn.f32x2 PTX,
+// while the scalar _rn operations are never contracted.
 struct F2 {
   float2 v;
 };
 __device__ __forceinline__ F2 pk(float a, float b) { return F2{make_float2(a, b)}; }
 __device__ __forceinline__ F2 fadd(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
-__device__ __forceinline__ F2 fmul(F2 a, F2 b) { return F2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ F2 fmul(F2 a, F2 b) {
+  return pk(__fmul_rn(a.v.x, b.v.x), __fmul_rn(a.v.y, b.v.y));
+}
 __device__ __forceinline__ F2 fsub(F2 a, F2 b) {
   unsigned long long ra, rb, rd;
   memcpy(&ra, &a.v, 8);

@@ -633,7 +633,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   const int s_cur = SCUR >= 0 ? SCUR : s_cur_rt;
   const int s_nxt = SNXT >= 0 ? SNXT : s_nxt_rt;
   // packed two-cell arithmetic in the compile-time tiles (V even)
-  constexpr bool PK = G::kFixed && (V % 2 == 0);
+  constexpr bool PK = (V % 2 == 0);
   if (*(volatile int*)&sh.abort_flag) return false;
   if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
     *(volatile int*)&sh.abort_flag = 1;

@@ -232,6 +232,38 @@ def _seed(ev, level, E):
             ev.set_psi_imag(0.25 * E)
 
 
+@pytest.mark.parametrize("N", [20, 24, 48, 128, 256])
+@pytest.mark.parametrize("level", ["real", "complex"])
+def test_resident_steps_bit_exact_at_every_kernel_shape(be, N, level):
+    """Resident steps against the float32 oracle at sizes that reach each kernel
+    variant: run-time tiles (24, 48), the direct fallback (20 COMPLEX), and the
+    compile-time tiles with packed two-cell arithmetic (128, 256)."""
+    from lfm_b200 import Evolver
+    from lfm_b200.config import gravity_em, gravity_only
+
+    cfg = (gravity_only if level == "real" else gravity_em)(N, boundary_fraction=0.3)
+    rng = np.random.default_rng(N + (7 if level == "complex" else 0))
+    E = (0.7 * rng.standard_normal((N, N, N))).astype(np.float32)
+    chi = (CHI0 + 0.05 * rng.standard_normal((N, N, N))).astype(np.float32)
+    ev = Evolver(cfg, backend=be)
+    lat = O.OracleLattice(cfg)
+    O.set_threads(O.max_threads())
+    for tgt in (ev, lat):
+        tgt.set_psi_real(E)
+        if level == "complex":
+            tgt.set_psi_imag(0.5 * E[::-1].copy())
+        tgt.set_chi(chi)
+    steps = 3
+    ev.use_graphs = False
+    ev.evolve(steps)
+    lat.step(steps)
+    assert bits_equal(ev.get_psi_real().ravel(), lat.pr)
+    assert bits_equal(ev.get_chi().ravel(), lat.chi)
+    assert bits_equal(ev.get_psi_real_prev().ravel(), lat.prp)
+    if level == "complex":
+        assert bits_equal(ev.get_psi_imag().ravel(), lat.pi)
+
+
 @pytest.mark.parametrize("buffers", ["resident", "ab"])
 @pytest.mark.parametrize("level", ["real", "complex"])
 def test_evolver_fifty_steps_match_reference_bit_exact(be, path, buffers, level):
