@@ -204,6 +204,27 @@ int lfm_poisson_chi_f32(lfm_context* ctx, int level, const float* psi_r, const f
                         int N, double chi0, double kappa, double e0_sq,
                         double boundary_fraction, int frozen, float* chi_out, void* stream);
 
+/* ------------------------------------------------------------------------
+ * One slab of a lattice split along i across GPUs (the natural sharding of a
+ * single large lattice; the reference steps the whole lattice on one device,
+ * lfm/core/backends/numpy_backend.py:80-205).  Level LFM_REAL or LFM_COMPLEX.
+ * Every array holds n_local + 2 planes of N x N: plane 0 and plane
+ * n_local + 1 are ghost copies of global planes i_first - 1 and
+ * i_first + n_local (mod N), planes 1 .. n_local are global planes
+ * i_first .. i_first + n_local - 1.  The step is the resident step of
+ * lfm_leapfrog_*_f32 restricted to planes 1 .. n_local: it reads the ghost
+ * planes of psi / chi as they are and writes the new fields over the
+ * previous ones.  The caller refreshes the ghost planes of the new fields
+ * (from the neighbouring slabs) before the next step.  The results are the
+ * whole-lattice step's bits on those planes.  psi_i* are ignored (may be
+ * NULL) at the REAL level.
+ * ------------------------------------------------------------------------ */
+int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                      float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                      const float* mask_table, const lfm_mask_lut* lut, int damp_prev, int N,
+                      int n_local, int i_first, double dt2, double kappa, double lambda_self,
+                      double chi0, double e0_sq, double epsilon_w, void* stream);
+
 /* Out-of-place form of lfm_leapfrog_real_f32 / lfm_leapfrog_complex_f32
  * (level LFM_REAL or LFM_COMPLEX): the same step and the same bits, with the
  * new fields written to *_out instead of over the previous ones, which stay

@@ -570,6 +570,52 @@ int lfm_poisson_chi_f32(lfm_context* ctx, int level, const float* psi_r, const f
   return LFM_OK;
 }
 
+int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                      float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                      const float* mask_table, const lfm_mask_lut* lut, int damp_prev, int N,
+                      int n_local, int i_first, double dt2, double kappa, double lambda_self,
+                      double chi0, double e0_sq, double epsilon_w, void* stream) {
+  if (level != LFM_REAL && level != LFM_COMPLEX)
+    return fail(LFM_ERR_UNSUPPORTED, "slab step: level %d (REAL and COMPLEX only)", level);
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (n_local < 1 || i_first < 0 || i_first + n_local > N)
+    return fail(LFM_ERR_INVALID_ARG, "slab planes [%d, %d) outside [0, %d)", i_first,
+                i_first + n_local, N);
+  const bool cx = level == LFM_COMPLEX;
+  if (!psi_r || !psi_r_prev_io || !chi || !chi_prev_io || (cx && (!psi_i || !psi_i_prev_io)))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)(n_local + 2) * N * N;
+  std::vector<Span> ins = {{psi_r, b}, {chi, b}};
+  std::vector<Span> outs = {{psi_r_prev_io, b}, {chi_prev_io, b}};
+  if (cx) {
+    ins.push_back({psi_i, b});
+    outs.push_back({psi_i_prev_io, b});
+  }
+  rc = check_disjoint(ins, outs);
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = level;
+  a.N = N;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, cx ? epsilon_w : 0.0, 0, 0,
+                              0, 0);
+  a.pr = psi_r; a.pr_prev = psi_r_prev_io; a.pr_out = psi_r_prev_io;
+  if (cx) {
+    a.pi = psi_i; a.pi_prev = psi_i_prev_io; a.pi_out = psi_i_prev_io;
+  }
+  a.chi = chi; a.chi_prev = chi_prev_io; a.chi_out = chi_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  a.slab = 1;
+  a.ni = n_local + 2;
+  a.i_lo = 1;
+  a.i_hi = n_local + 1;
+  a.i_off = i_first - 1;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
 int lfm_advance_f32(int level, const float* psi_r, const float* psi_r_prev, float* psi_r_out,
                     const float* psi_i, const float* psi_i_prev, float* psi_i_out,
                     const float* chi, const float* chi_prev, float* chi_out,

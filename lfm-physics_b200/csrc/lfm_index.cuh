@@ -31,6 +31,26 @@ __device__ __forceinline__ Idx neighbour_index(int i, int j, int k, int N) {
   return x;
 }
 
+// The same neighbourhood in a slab array: planes i-1 and i+1 are read as they
+// are (ghost planes hold the neighbours' data), j and k wrap.
+__device__ __forceinline__ Idx neighbour_index_slab(int i, int j, int k, int N) {
+  const int64_t n = N;
+  const int64_t im = i - 1, ip = i + 1;
+  const int64_t jm = (j == 0 ? N - 1 : j - 1), jp = (j == N - 1 ? 0 : j + 1);
+  const int64_t km = (k == 0 ? N - 1 : k - 1), kp = (k == N - 1 ? 0 : k + 1);
+  const int64_t I0 = im * n * n, I1 = (int64_t)i * n * n, I2 = ip * n * n;
+  const int64_t J0 = jm * n, J1 = (int64_t)j * n, J2 = jp * n;
+  Idx x;
+  x.c = I1 + J1 + k;
+  x.im = I0 + J1 + k;   x.ip = I2 + J1 + k;
+  x.jm = I1 + J0 + k;   x.jp = I1 + J2 + k;
+  x.km = I1 + J1 + km;  x.kp = I1 + J1 + kp;
+  x.imjm = I0 + J0 + k; x.imjp = I0 + J2 + k; x.ipjm = I2 + J0 + k; x.ipjp = I2 + J2 + k;
+  x.imkm = I0 + J1 + km; x.imkp = I0 + J1 + kp; x.ipkm = I2 + J1 + km; x.ipkp = I2 + J1 + kp;
+  x.jmkm = I1 + J0 + km; x.jmkp = I1 + J0 + kp; x.jpkm = I1 + J2 + km; x.jpkp = I1 + J2 + kp;
+  return x;
+}
+
 __device__ __forceinline__ S19 gather(const float* __restrict__ f, const Idx& x) {
   S19 s;
   s.c = __ldg(f + x.c);

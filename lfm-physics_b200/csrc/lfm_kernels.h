@@ -35,6 +35,12 @@ struct StepArgs {
   int damp_prev;       // multiply the previous-step fields by (1-mask) on read
   int comp;            // compensated Delta form: *_prev hold increments, updated in place
   int* status;         // device status word for bounded waits
+  // Slab of a lattice split along i (slab == 0: the whole periodic lattice).
+  // The arrays hold ni planes of N x N; the step updates planes [i_lo, i_hi)
+  // and reads planes i_lo - 1 and i_hi as they are (ghost planes, no wrap);
+  // array plane p is global plane p + i_off (for the sponge).
+  int slab;
+  int ni, i_lo, i_hi, i_off;
 };
 
 cudaError_t launch_direct_step(const StepArgs& a, cudaStream_t stream);

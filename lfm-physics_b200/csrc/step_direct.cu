@@ -19,7 +19,7 @@ __device__ __forceinline__ Faces faces_of(const S19& s) {
 
 __device__ __forceinline__ float cell_mask(const StepArgs& a, int i, int j, int k, int64_t x) {
   if (a.mask) return __ldg(a.mask + x);
-  return mask_from_q(a.lut, qterm(i, a.N) + qterm(j, a.N) + qterm(k, a.N));
+  return mask_from_q(a.lut, qterm(i + a.i_off, a.N) + qterm(j, a.N) + qterm(k, a.N));
 }
 
 // Previous-step value: slots written by the previous resident step hold the
@@ -35,12 +35,16 @@ template <int LEVEL>
 __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
   const int N = a.N;
   const int64_t n3 = (int64_t)N * N * N;
-  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n3;
-       x += (int64_t)gridDim.x * blockDim.x) {
+  // a slab updates planes [i_lo, i_hi) of its array and reads i_lo-1, i_hi
+  const int64_t first = a.slab ? (int64_t)a.i_lo * N * N : 0;
+  const int64_t count = a.slab ? (int64_t)(a.i_hi - a.i_lo) * N * N : n3;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = first + t;
     const int k = (int)(x % N);
     const int j = (int)((x / N) % N);
     const int i = (int)(x / ((int64_t)N * N));
-    const Idx ix = neighbour_index(i, j, k, N);
+    const Idx ix = a.slab ? neighbour_index_slab(i, j, k, N) : neighbour_index(i, j, k, N);
     const float mask = cell_mask(a, i, j, k, x);
     const float absorb = fsub(1.0f, mask);
     const S19 X = gather(a.chi, ix);
@@ -130,7 +134,7 @@ __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
 }  // namespace
 
 cudaError_t launch_direct_step(const StepArgs& a, cudaStream_t stream) {
-  const int64_t n3 = (int64_t)a.N * a.N * a.N;
+  const int64_t n3 = a.slab ? (int64_t)(a.i_hi - a.i_lo) * a.N * a.N : (int64_t)a.N * a.N * a.N;
   const int block = 256;
   int64_t blocks = (n3 + block - 1) / block;
   const int64_t cap = 148LL * 16;  // grid-stride beyond 16 waves of CTAs

@@ -389,11 +389,12 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
 }
 
 // Copies plane (i0 - 1 + u) into stage u % S.
+template <bool SLAB = true>
 __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                             int u, int i0, int i1, int j0) {
   const int N = P.N, TJ = P.TJ;
   const int p = i0 - 1 + u;
-  const int pw = (p % N + N) % N;
+  const int pw = (SLAB && P.a.slab) ? p : (p % N + N) % N;  // slabs read their ghost planes
   const int s = u % P.S;
   float* st = smem + (size_t)s * P.stage_floats;
   const bool point = (p >= i0) && (p < i1);
@@ -587,6 +588,7 @@ struct QFields {
 // offset of a plane folds into an immediate beside one per-thread base.
 struct GeomRT {
   static constexpr bool kFixed = false;
+  static constexpr bool kSlab = true;  // may step a slab (plane range, ghost planes)
   int N, TJ, S, SF;
   __device__ __forceinline__ explicit GeomRT(const TmaParams& P)
       : N(P.N), TJ(P.TJ), S(P.S), SF(P.stage_floats) {}
@@ -595,6 +597,7 @@ struct GeomRT {
 template <int N_, int TJ_, int NS_>
 struct GeomCT {
   static constexpr bool kFixed = true;
+  static constexpr bool kSlab = false;  // whole lattices only
   static constexpr int N = N_, TJ = TJ_, S = 3, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
   __device__ __forceinline__ explicit GeomCT(const TmaParams&) {}
 };
@@ -659,7 +662,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   } else if constexpr (G::kFixed) {
     // table values of this plane were fetched one plane ago; fetch the next
     // plane's now, so their latency overlaps this plane's arithmetic
-    const int32_t qij = qterm(i, N) + K.qj;
+    const int32_t qij = qterm(i, N) + K.qj;  // fixed geometry: whole lattices
 #pragma unroll
     for (int e = 0; e < V; ++e) mask[e] = mask_pick(a.lut, qij + K.qk[e], mraw[e]);
     if (c + 1 < i1 - i0) {
@@ -668,7 +671,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       for (int e = 0; e < V; ++e) mraw[e] = mask_fetch(a.lut, qn + K.qk[e]);
     }
   } else {
-    q_mask<V>(a.lut, qterm(i, N), K, mask);
+    q_mask<V>(a.lut, qterm(i + (G::kSlab ? a.i_off : 0), N), K, mask);
   }
 #pragma unroll
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
@@ -814,7 +817,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       sh.done[s_cur] = 0u;
       fence_proxy_async_smem();
       if (c + 1 + P.S < nplanes) {
-        issue_plane(P, smem, bars, c + 1 + P.S, i0, i1, j0);
+        issue_plane<G::kSlab>(P, smem, bars, c + 1 + P.S, i0, i1, j0);
         atomicMax(&sh.issued, c + 2 + P.S);
       }
     }
@@ -880,7 +883,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   __syncthreads();
   if (tid == 0) {
     const int first = min(S, nplanes);
-    for (int u = 0; u < first; ++u) issue_plane(P, smem, bars, u, i0, i1, j0);
+    for (int u = 0; u < first; ++u) issue_plane<G::kSlab>(P, smem, bars, u, i0, i1, j0);
     sh.issued = first;
   }
   QPlane<V> Q[NS][3];
@@ -912,7 +915,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     // stage 0 (plane i0-1) is dead: refill it with u = S
     if (tid == 0 && S < nplanes) {
       fence_proxy_async_smem();
-      issue_plane(P, smem, bars, S, i0, i1, j0);
+      issue_plane<G::kSlab>(P, smem, bars, S, i0, i1, j0);
       sh.issued = S + 1;
     }
     int s_cur = 1 % S, s_nxt = 2 % S;
@@ -953,8 +956,10 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
   __shared__ QShared sh;
   const G g(P);
   const int jt = blockIdx.x % P.JT, ch = blockIdx.x / P.JT;
-  const int i0 = ch * P.IC;
-  q_march<LEVEL, V, COMP, false, G>(P, smem, bars, sh, jt * g.TJ, i0, min(i0 + P.IC, g.N), g.TJ);
+  const bool slab = G::kSlab && P.a.slab;
+  const int lo = slab ? P.a.i_lo : 0, hi = slab ? P.a.i_hi : g.N;
+  const int i0 = lo + ch * P.IC;
+  q_march<LEVEL, V, COMP, false, G>(P, smem, bars, sh, jt * g.TJ, i0, min(i0 + P.IC, hi), g.TJ);
 }
 
 // ---- batch kernel: many lattices, one launch per step -------------------------
@@ -1085,7 +1090,8 @@ int carveout_kb(int bytes) {
 // when it is staged there); l1_table_bytes: a table read through L1 that the
 // carveout must leave room for (0 when none).
 Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threads,
-              int regs, const TileConfig* forced, int extra_smem, int l1_table_bytes) {
+              int regs, const TileConfig* forced, int extra_smem, int l1_table_bytes, int planes = 0) {
+  if (planes <= 0) planes = N;  // planes the march covers (a slab's own planes)
   Choice best;
   double best_score = -1.0;
   const int tpr = N / V;
@@ -1125,7 +1131,7 @@ Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threa
                                                  2048 / best.threads),
                                         65536 / std::max(1, regs * best.threads)));
   if (forced && forced->ic > 0) {
-    best.IC = std::min(forced->ic, N);
+    best.IC = std::min(forced->ic, planes);
   } else {
     // Planes per chunk: minimise waves x (pipeline fill + (IC + 2) planes).
     // A CTA streams one plane of TJ x N cells in t_plane, no faster than the
@@ -1139,8 +1145,8 @@ Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threa
     const double t_plane = std::max((double)best.TJ * N * ctas / r_sm,
                                     t_lat / std::max(1, best.S - (min_s - 1)));
     double best_t = 1e300;
-    for (int chunks = 1; chunks <= std::max(1, N / 2); ++chunks) {
-      const int ic = (N + chunks - 1) / chunks;
+    for (int chunks = 1; chunks <= std::max(1, planes / 2); ++chunks) {
+      const int ic = (planes + chunks - 1) / chunks;
       const double waves = std::ceil((double)JT * chunks / slots);
       const double t = waves * (t_fill + (ic + 2) * t_plane);
       if (t < best_t * (1.0 - 1e-9)) {
@@ -1182,7 +1188,8 @@ cudaError_t launch_kernel(K kernel, int* granted, std::mutex* mu, const TmaParam
     }
   }
   const int JT = P.N / P.TJ;
-  const int chunks = (P.N + P.IC - 1) / P.IC;
+  const int planes = P.a.slab ? P.a.i_hi - P.a.i_lo : P.N;
+  const int chunks = (planes + P.IC - 1) / P.IC;
   kernel<<<JT * chunks, ch.threads, ch.smem, stream>>>(P);
   return cudaGetLastError();
 }
@@ -1239,7 +1246,7 @@ cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
 // kFixedTiles (3 stages, no streamed mask or S_a); false if there is none.
 template <int LEVEL, int V>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
-  if (ch.S != 3 || P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0) return false;
+  if (ch.S != 3 || P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
   const FixedTile* t = fixed_tile(LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ) return false;
   if constexpr (LEVEL == LFM_REAL && V == 4) {
@@ -1270,14 +1277,15 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // Without a forced tile, the sizes with a compile-time variant take its
   // tile (TJ rows, 3 stages); the planner still picks the plane chunk.
   TileConfig fixed_cfg;
-  const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns)
+  const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns &&
+                         !P.a.slab)
                             ? fixed_tile(LEVEL, V, P.N) : nullptr;
   if (!forced && ft) {
     fixed_cfg = TileConfig{ft->TJ, 3, 0, 0, 0, V};
     forced = &fixed_cfg;
   }
   const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0,
-                           table_bytes);
+                           table_bytes, P.a.slab ? P.a.i_hi - P.a.i_lo : P.N);
   if (!ch.TJ) return cudaErrorNotSupported;
   P.TJ = ch.TJ;
   P.S = ch.S;
