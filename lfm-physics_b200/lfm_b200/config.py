@@ -48,6 +48,37 @@ VOID_THRESHOLD = 18.0
 E_AMPLITUDE_BY_GRID = {32: 12.0, 64: 6.0, 128: 3.6, 256: 1.8, 512: 0.9}
 
 
+# Physical radius of the observable universe in Planck lengths: the default
+# box_planck_radius (metadata only; lfm/constants.py:238-254).
+PLANCK_TIME_SEC = 5.391e-44
+AGE_UNIVERSE_GYR = 13.8
+SEC_PER_GYR = 1e9 * 365.25 * 24 * 3600
+OBSERVABLE_RADIUS_PLANCK = (AGE_UNIVERSE_GYR * SEC_PER_GYR) / PLANCK_TIME_SEC
+
+
+class ChiMode(enum.Enum):
+    """GOV-02 update rule named by the config (lfm/config.py:49-67).  The step
+    kernels implement WAVE, the full second-order chi equation."""
+
+    WAVE = "wave"
+    MEMORY = "memory"
+    STATIC = "static"
+
+
+class PhysicsScale(enum.Enum):
+    """Named physical scale (lfm/config.py:70-129); setting one on the config
+    selects the field level, chi mode and couplings below."""
+
+    PLANCK = "planck"
+    NUCLEAR = "nuclear"
+    ATOMIC = "atomic"
+    MOLECULAR = "molecular"
+    CLASSICAL = "classical"
+    SOLAR = "solar"
+    GALACTIC = "galactic"
+    COSMIC = "cosmic"
+
+
 class FieldLevel(enum.IntEnum):
     """Field representation: real E, one complex Psi, or three colour components."""
 
@@ -66,6 +97,18 @@ class BoundaryType(enum.Enum):
     FROZEN = "frozen"
     PERIODIC = "periodic"
     ABSORBING = "absorbing"
+
+
+_SCALE_DEFAULTS = {
+    PhysicsScale.PLANCK: (FieldLevel.COLOR, ChiMode.WAVE, LAMBDA_H, KAPPA_C),
+    PhysicsScale.NUCLEAR: (FieldLevel.COLOR, ChiMode.WAVE, LAMBDA_H, KAPPA_C),
+    PhysicsScale.ATOMIC: (FieldLevel.COMPLEX, ChiMode.WAVE, 0.0, 0.0),
+    PhysicsScale.MOLECULAR: (FieldLevel.COMPLEX, ChiMode.WAVE, 0.0, 0.0),
+    PhysicsScale.CLASSICAL: (FieldLevel.REAL, ChiMode.WAVE, 0.0, 0.0),
+    PhysicsScale.SOLAR: (FieldLevel.REAL, ChiMode.WAVE, 0.0, 0.0),
+    PhysicsScale.GALACTIC: (FieldLevel.REAL, ChiMode.MEMORY, 0.0, 0.0),
+    PhysicsScale.COSMIC: (FieldLevel.REAL, ChiMode.MEMORY, 0.0, 0.0),
+}
 
 
 @dataclass
@@ -92,12 +135,24 @@ class SimulationConfig:
     boundary_fraction: float = BOUNDARY_FRACTION_DEFAULT
     e_amplitude: float = 0.0
     blob_sigma_factor: float = 12.0
+    phase1_steps: int = 10_000
+    phase1_omega: float = 38.0
+    phase1_amplitude: float = 0.3
     random_seed: int = 42
     report_interval: int = 5000
+    box_planck_radius: float = OBSERVABLE_RADIUS_PLANCK
+    physical_scale: PhysicsScale | None = None
+    chi_mode: ChiMode = ChiMode.WAVE
     dx: float = field(init=False, default=1.0)
     sigma: float = field(init=False, default=0.0)
 
     def __post_init__(self) -> None:
+        if self.physical_scale is not None:
+            self.physical_scale = PhysicsScale(self.physical_scale)
+            fl, cm, ls, kc = _SCALE_DEFAULTS[self.physical_scale]
+            self.field_level, self.chi_mode, self.lambda_self, self.kappa_c = fl, cm, ls, kc
+        if not isinstance(self.chi_mode, ChiMode):
+            self.chi_mode = ChiMode(self.chi_mode)
         self.field_level = FieldLevel(int(self.field_level))
         if not isinstance(self.boundary_type, BoundaryType):
             self.boundary_type = BoundaryType(self.boundary_type)

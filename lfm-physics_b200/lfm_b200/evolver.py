@@ -400,6 +400,25 @@ class Evolver:
             return None
         return self._shape(self._to_host(self._prev_psi_view(True)))
 
+    def get_chi_prev(self) -> np.ndarray:
+        """Previous-step chi as the next step reads it, (N, N, N)."""
+        return self._to_host(self._active("chi_prev")).reshape(self.N, self.N, self.N)
+
+    def save_checkpoint(self, path, history=None, psi_snapshot=None) -> None:
+        """npz checkpoint in the reference's format plus the leapfrog previous
+        fields (lfm_b200.checkpoint): loading it resumes bit for bit."""
+        from .checkpoint import save_checkpoint
+
+        save_checkpoint(self, path, history=history, psi_snapshot=psi_snapshot)
+
+    @classmethod
+    def load_checkpoint(cls, path, backend="auto", buffers: str = "resident") -> "Evolver":
+        """An Evolver restored from a checkpoint written by save_checkpoint or
+        by the reference's Simulation.save_checkpoint."""
+        from .checkpoint import load_checkpoint
+
+        return load_checkpoint(path, backend=backend, buffers=buffers)[0]
+
     def get_energy_density(self) -> np.ndarray:
         pr = self.get_psi_real()
         e2 = np.sum(pr**2, axis=0) if pr.ndim == 4 else pr**2

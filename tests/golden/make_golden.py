@@ -240,6 +240,18 @@ def sweep_fixture() -> None:
     np.savez_compressed(OUT / "sweep.npz", runs=np.array(json.dumps(runs)))
 
 
+def checkpoint_fixture() -> None:
+    """A checkpoint written by the reference's Simulation (NumPy backend)."""
+    from lfm.config_presets import gravity_em
+    from lfm.simulation import Simulation
+
+    sim = Simulation(gravity_em(12), backend="cpu")
+    sim.place_soliton((6, 5, 6), amplitude=3.0, sigma=1.5, phase=0.4)
+    sim.equilibrate()
+    sim.run(steps=4, record_metrics=False)
+    sim.save_checkpoint(OUT / "ref_checkpoint.npz")
+
+
 if __name__ == "__main__":
     masks()
     stencil()
@@ -249,4 +261,5 @@ if __name__ == "__main__":
     config1()
     equilibrium_fixture()
     sweep_fixture()
+    checkpoint_fixture()
     print("fixtures written to", OUT)
