@@ -18,22 +18,30 @@ struct RealOutT {
 };
 using RealOut = RealOutT<float>;
 
+// absorb = 1 - mask, passed in by kernels that also damp the stored
+// previous field with it (one subtraction per cell instead of two).
 template <class T>
-__device__ __forceinline__ RealOutT<T> real_cell(T lapE, T e, T e_prev, T lapX, T chi,
-                                                 T chi_prev, T mask, const StepConsts& s) {
+__device__ __forceinline__ RealOutT<T> real_cell_ab(T lapE, T e, T e_prev, T lapX, T chi,
+                                                    T chi_prev, T mask, T absorb,
+                                                    const StepConsts& s) {
   const T chi_sq = fmul(chi, chi);
   const T E_new = gov01(e, e_prev, lapE, chi_sq, s);
   // chi_source = (kappa/chi0)*chi*(E*E - e0_sq)
   const T src = fmul(fmul(cst<T>(s.k_over_chi0), chi), fsub(fmul(e, e), cst<T>(s.e0_sq)));
   T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
-  const T absorb = fsub(cst<T>(1.0f), mask);
   RealOutT<T> o;
   o.psi = fmul(E_new, absorb);
   o.psi_prev = fmul(e, absorb);
   o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
   o.chi_prev = chi;
   return o;
+}
+
+template <class T>
+__device__ __forceinline__ RealOutT<T> real_cell(T lapE, T e, T e_prev, T lapX, T chi,
+                                                 T chi_prev, T mask, const StepConsts& s) {
+  return real_cell_ab(lapE, e, e_prev, lapX, chi, chi_prev, mask, fsub(cst<T>(1.0f), mask), s);
 }
 
 // ---- COMPLEX (numpy_backend.py:132-205) -----------------------------------
@@ -68,11 +76,11 @@ __device__ __forceinline__ T momentum_current(T pr, T pi, const FacesT<T>& R,
 }
 
 template <class T>
-__device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
-                                                       const FacesT<T>& R, T lapI, T pi,
-                                                       T pi_prev, const FacesT<T>& I, T lapX,
-                                                       T chi, T chi_prev, T mask,
-                                                       const StepConsts& s) {
+__device__ __forceinline__ ComplexOutT<T> complex_cell_ab(T lapR, T pr, T pr_prev,
+                                                          const FacesT<T>& R, T lapI, T pi,
+                                                          T pi_prev, const FacesT<T>& I, T lapX,
+                                                          T chi, T chi_prev, T mask, T absorb,
+                                                          const StepConsts& s) {
   const T chi_sq = fmul(chi, chi);
   const T Pr_new = gov01(pr, pr_prev, lapR, chi_sq, s);
   const T Pi_new = gov01(pi, pi_prev, lapI, chi_sq, s);
@@ -83,7 +91,6 @@ __device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
                      fsub(fadd(psi_sq, fmul(cst<T>(s.eps_w), jt)), cst<T>(s.e0_sq)));
   T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
-  const T absorb = fsub(cst<T>(1.0f), mask);
   ComplexOutT<T> o;
   o.pr = fmul(Pr_new, absorb);
   o.pi = fmul(Pi_new, absorb);
@@ -92,6 +99,16 @@ __device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
   o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
   o.chi_prev = chi;
   return o;
+}
+
+template <class T>
+__device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
+                                                       const FacesT<T>& R, T lapI, T pi,
+                                                       T pi_prev, const FacesT<T>& I, T lapX,
+                                                       T chi, T chi_prev, T mask,
+                                                       const StepConsts& s) {
+  return complex_cell_ab(lapR, pr, pr_prev, R, lapI, pi, pi_prev, I, lapX, chi, chi_prev, mask,
+                         fsub(cst<T>(1.0f), mask), s);
 }
 
 // ---- COLOR (numpy_backend.py:207-382), three colours ----------------------

@@ -32,9 +32,24 @@ struct F2 {
 };
 __device__ __forceinline__ F2 pk(float a, float b) { return F2{make_float2(a, b)}; }
 __device__ __forceinline__ F2 fadd(F2 a, F2 b) { return F2{__fadd2_rn(a.v, b.v)}; }
+#ifdef LFM_PACKED_MUL_FMA
+// a*b as fma(a, b, -0): one rounding of the exact product (a -0 addend leaves
+// every product, signed zeros included, unchanged).
+__device__ __forceinline__ F2 fmul(F2 a, F2 b) {
+  unsigned long long ra, rb, rd;
+  const unsigned long long nz = 0x8000000080000000ull;
+  memcpy(&ra, &a.v, 8);
+  memcpy(&rb, &b.v, 8);
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(rd) : "l"(ra), "l"(rb), "l"(nz));
+  F2 d;
+  memcpy(&d.v, &rd, 8);
+  return d;
+}
+#else
 __device__ __forceinline__ F2 fmul(F2 a, F2 b) {
   return pk(__fmul_rn(a.v.x, b.v.x), __fmul_rn(a.v.y, b.v.y));
 }
+#endif
 __device__ __forceinline__ F2 fsub(F2 a, F2 b) {
   unsigned long long ra, rb, rd;
   memcpy(&ra, &a.v, 8);
@@ -139,10 +154,18 @@ __device__ __forceinline__ float lap19(const S19& f) {
 // The pointwise helpers below take T = float (one cell) or F2 (two cells,
 // packed); both evaluate the same operations in the same order per cell.
 
+// 2.0*x, as x + x: doubling is exact in binary floating point (x + x and
+// 2*x give the same bits for every x, zeros, infinities and NaN included),
+// and for two cells the addition is one packed FADD2.
+template <class T>
+__device__ __forceinline__ T twice(T x) {
+  return fadd(x, x);
+}
+
 // GOV-01: 2.0*P - P_prev + dt2*(lap - chi_sq*P)   (numpy_backend.py:108)
 template <class T>
 __device__ __forceinline__ T gov01(T p, T p_prev, T lap, T chi_sq, const StepConsts& s) {
-  return fadd(fsub(fmul(cst<T>(2.0f), p), p_prev), fmul(cst<T>(s.dt2), fsub(lap, fmul(chi_sq, p))));
+  return fadd(fsub(twice(p), p_prev), fmul(cst<T>(s.dt2), fsub(lap, fmul(chi_sq, p))));
 }
 
 // chi_accel -= 4*lambda*chi*(chi^2 - chi0^2) when lambda > 0 (numpy_backend.py:113-114)
@@ -157,7 +180,7 @@ __device__ __forceinline__ T mexican_hat(T acc, T chi, T chi_sq, const StepConst
 template <class T>
 __device__ __forceinline__ T gov02_finish(T chi, T chi_prev, T acc, T mask, T absorb,
                                           const StepConsts& s) {
-  T chi_new = fadd(fsub(fmul(cst<T>(2.0f), chi), chi_prev), fmul(cst<T>(s.dt2), acc));
+  T chi_new = fadd(fsub(twice(chi), chi_prev), fmul(cst<T>(s.dt2), acc));
   chi_new = clamp_below(chi_new, s.neg_chi0);
   return fadd(fmul(mask, cst<T>(s.chi0)), fmul(absorb, chi_new));
 }
@@ -217,20 +240,6 @@ __device__ __forceinline__ float mask_from_q_flat(const MaskLut& m, int32_t q) {
   const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
   float t = 0.0f;
   if (in_band) t = __ldg(m.table + ((q - m.q_lo) >> m.shift));
-  return in_band ? t : (q < m.q_lo ? 0.0f : 1.0f);
-}
-
-// mask_from_q_flat in two halves, so that a kernel can issue a cell's table
-// load one plane early and pick the value when it needs it:
-// mask_pick(m, q, mask_fetch(m, q)) == mask_from_q_flat(m, q).
-__device__ __forceinline__ float mask_fetch(const MaskLut& m, int32_t q) {
-  const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
-  float t = 0.0f;
-  if (in_band) t = __ldg(m.table + ((q - m.q_lo) >> m.shift));
-  return t;
-}
-__device__ __forceinline__ float mask_pick(const MaskLut& m, int32_t q, float t) {
-  const bool in_band = (q >= m.q_lo) & (q <= m.q_hi);
   return in_band ? t : (q < m.q_lo ? 0.0f : 1.0f);
 }
 

@@ -68,6 +68,13 @@ __device__ __forceinline__ void mbar_init_fence() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Raises the barrier's expected transaction bytes without arriving.
+__device__ __forceinline__ void mbar_add_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes)
@@ -508,12 +515,46 @@ struct QLane {
   int o_pt;                                // point rows at k0 (from the stage base)
 };
 
-// Radial keys of a thread's cells: q = qterm(i) + qj + qk[e].
+// Radial keys of a thread's cells: q = qterm(i) + qj + qk[e].  The
+// compile-time tiles use byte offsets into the shared-memory sponge table
+// instead: offset = min_relu(4*key8(i) + aj4 + ak4[e], cap4) (see sponge_key).
 template <int V>
 struct QKeys {
   int32_t qj;
   int32_t qk[V];
+  int32_t aj4, cap4;
+  int32_t ak4[V];
 };
+
+// (qterm(x, N) - 1) / 8 for even N.  qterm is an odd square, 1 mod 8, so a
+// cell's key q = 8 * (key8(i) + key8(j) + key8(k)) + 3 exactly, and q >> 3 is
+// the sum of the three.
+__device__ __forceinline__ int32_t key8(int x, int N) { return (qterm(x, N) - 1) >> 3; }
+
+// max(min(a, b), 0) in one instruction.
+__device__ __forceinline__ int32_t min_relu(int32_t a, int32_t b) {
+  int32_t d;
+  asm("min.relu.s32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// The sponge table in shared memory, for the compile-time tiles:
+//   tab[0] = 0, tab[1 + t] = lut.table[t] (t < count), tab[count + 1] = 1,
+// with tab[1] on a 16-byte boundary so the copy engine can fill it.
+// A cell's entry is t = q/8 - q_lo/8 + 1 clamped to [0, count + 1]: keys below
+// the band land on the 0, keys above it on the 1, so the lookup needs no band
+// test and no select.  (q_lo - 3) >> 3 also covers the two empty bands: the
+// all-zero mask (q_lo = INT32_MAX, every offset clamps to 0) and the all-one
+// mask (q_lo = 0, count = 0, every offset clamps to 1).
+template <int V>
+__device__ __forceinline__ void sponge_key(QKeys<V>& K, const MaskLut& lut, int j, int k0,
+                                           int N) {
+  const int32_t key_lo = (lut.q_lo - 3) >> 3;
+  K.aj4 = 4 * (key8(j, N) + 1 - key_lo);
+  K.cap4 = 4 * (lut.count + 1);
+#pragma unroll
+  for (int e = 0; e < V; ++e) K.ak4[e] = 4 * key8(k0 + e, N);
+}
 
 // Mask values of a thread's cells.  The table load is predicated on the band
 // test (mask_from_q_flat): a branch around whole rows inside or beyond the
@@ -589,16 +630,20 @@ struct QFields {
 struct GeomRT {
   static constexpr bool kFixed = false;
   static constexpr bool kSlab = true;  // may step a slab (plane range, ghost planes)
+  static constexpr int kStages = 0;    // stage count known at run time only
   int N, TJ, S, SF;
   __device__ __forceinline__ explicit GeomRT(const TmaParams& P)
       : N(P.N), TJ(P.TJ), S(P.S), SF(P.stage_floats) {}
 };
 
-template <int N_, int TJ_, int NS_>
+template <int N_, int TJ_, int NS_, int S_ = 3>
 struct GeomCT {
+  static_assert(N_ % 2 == 0, "the sponge keys of the compile-time tiles assume even N");
   static constexpr bool kFixed = true;
   static constexpr bool kSlab = false;  // whole lattices only
-  static constexpr int N = N_, TJ = TJ_, S = 3, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
+  static constexpr int kStages = S_;
+  static constexpr int N = N_, TJ = TJ_, S = S_, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
+  static constexpr int TAB = S * SF + 3;  // float offset of the sponge table's tab[0]
   __device__ __forceinline__ explicit GeomCT(const TmaParams&) {}
 };
 
@@ -623,7 +668,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
                                         const QLane& L, int c, int i0, int i1, int j0,
                                         int nplanes, int nwarps, int& s_cur_rt, int& s_nxt_rt,
                                         uint32_t& ph_nxt, const QKeys<V>& K,
-                                        bool lane_active, float (&mraw)[V]) {
+                                        bool lane_active) {
   // PARTIAL: the CTA may be wider than the tile (batch kernel)
   const bool active = !PARTIAL || lane_active;
   constexpr int NS = QFields<LEVEL>::ns;
@@ -660,16 +705,12 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
 #pragma unroll
     for (int e = 0; e < V; ++e) mask[e] = m.v[e];
   } else if constexpr (G::kFixed) {
-    // table values of this plane were fetched one plane ago; fetch the next
-    // plane's now, so their latency overlaps this plane's arithmetic
-    const int32_t qij = qterm(i, N) + K.qj;  // fixed geometry: whole lattices
+    // the shared-memory table with its clamped key (sponge_key)
+    const int32_t b4 = 4 * key8(i, N) + K.aj4;
+    const char* tab = reinterpret_cast<const char*>(smem + G::TAB);
 #pragma unroll
-    for (int e = 0; e < V; ++e) mask[e] = mask_pick(a.lut, qij + K.qk[e], mraw[e]);
-    if (c + 1 < i1 - i0) {
-      const int32_t qn = qterm(i + 1, N) + K.qj;
-#pragma unroll
-      for (int e = 0; e < V; ++e) mraw[e] = mask_fetch(a.lut, qn + K.qk[e]);
-    }
+    for (int e = 0; e < V; ++e)
+      mask[e] = *reinterpret_cast<const float*>(tab + min_relu(b4 + K.ak4[e], K.cap4));
   } else {
     q_mask<V>(a.lut, qterm(i + (G::kSlab ? a.i_off : 0), N), K, mask);
   }
@@ -730,11 +771,13 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
         const S19 E1 = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e + 1);
         const S19 X0 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
         const S19 X1 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e + 1);
+        const F2 mk = pk(mask[e], mask[e + 1]);
+        const F2 ab = fsub(cst<F2>(1.0f), mk);
         F2 epv = pk(ep.v[e], ep.v[e + 1]);
-        if (a.damp_prev) epv = fmul(epv, pk(absorb[e], absorb[e + 1]));
+        if (a.damp_prev) epv = fmul(epv, ab);
         const RealOutT<F2> o =
-            real_cell(lap19_pair(E0, E1), pk(E0.c, E1.c), epv, lap19_pair(X0, X1),
-                      pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]), pk(mask[e], mask[e + 1]), a.c);
+            real_cell_ab(lap19_pair(E0, E1), pk(E0.c, E1.c), epv, lap19_pair(X0, X1),
+                         pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]), mk, ab, a.c);
         o_psi[e] = o.psi.v.x; o_psi[e + 1] = o.psi.v.y;
         o_chi[e] = o.chi.v.x; o_chi[e + 1] = o.chi.v.y;
         o_pp[e] = o.psi_prev.v.x; o_pp[e + 1] = o.psi_prev.v.y;
@@ -768,17 +811,17 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
         const S19 I1 = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e + 1);
         const S19 X0 = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
         const S19 X1 = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e + 1);
+        const F2 mk = pk(mask[e], mask[e + 1]);
+        const F2 ab = fsub(cst<F2>(1.0f), mk);
         F2 rpv = pk(rp.v[e], rp.v[e + 1]), ipv = pk(ip.v[e], ip.v[e + 1]);
         if (a.damp_prev) {
-          const F2 ab = pk(absorb[e], absorb[e + 1]);
           rpv = fmul(rpv, ab);
           ipv = fmul(ipv, ab);
         }
-        const ComplexOutT<F2> o = complex_cell(
+        const ComplexOutT<F2> o = complex_cell_ab(
             lap19_pair(R0, R1), pk(R0.c, R1.c), rpv, pk_faces(faces_of(R0), faces_of(R1)),
             lap19_pair(I0, I1), pk(I0.c, I1.c), ipv, pk_faces(faces_of(I0), faces_of(I1)),
-            lap19_pair(X0, X1), pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]),
-            pk(mask[e], mask[e + 1]), a.c);
+            lap19_pair(X0, X1), pk(X0.c, X1.c), pk(xp.v[e], xp.v[e + 1]), mk, ab, a.c);
         o_r[e] = o.pr.v.x; o_r[e + 1] = o.pr.v.y;
         o_i[e] = o.pi.v.x; o_i[e + 1] = o.pi.v.y;
         o_c[e] = o.chi.v.x; o_c[e + 1] = o.chi.v.y;
@@ -816,9 +859,9 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     if (before == (uint32_t)(nwarps - 1)) {
       sh.done[s_cur] = 0u;
       fence_proxy_async_smem();
-      if (c + 1 + P.S < nplanes) {
-        issue_plane<G::kSlab>(P, smem, bars, c + 1 + P.S, i0, i1, j0);
-        atomicMax(&sh.issued, c + 2 + P.S);
+      if (c + 1 + g.S < nplanes) {
+        issue_plane<G::kSlab>(P, smem, bars, c + 1 + g.S, i0, i1, j0);
+        atomicMax(&sh.issued, c + 2 + g.S);
       }
     }
   }
@@ -827,7 +870,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
     if (SNXT == 2) ph_nxt ^= 1u;  // the next plane's stage wraps to 0
   } else {
     s_cur_rt = s_nxt_rt;
-    s_nxt_rt = (s_nxt_rt + 1 == P.S) ? 0 : s_nxt_rt + 1;
+    s_nxt_rt = (s_nxt_rt + 1 == g.S) ? 0 : s_nxt_rt + 1;
     if (s_nxt_rt == 0) ph_nxt ^= 1u;
   }
   return true;
@@ -869,6 +912,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   K.qj = qterm(j0 + r, N);
 #pragma unroll
   for (int e = 0; e < V; ++e) K.qk[e] = qterm(k0 + e, N);
+  if constexpr (G::kFixed) sponge_key<V>(K, P.a.lut, j0 + r, k0, N);
 
   __syncthreads();  // a previous march in this CTA is over in every warp
   if (tid == 0) {
@@ -881,22 +925,36 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     mbar_init_fence();
   }
   __syncthreads();
+  // floats of the sponge table the copy engine moves (compile-time tiles):
+  // whole 16-byte groups of a 16-byte aligned table
+  int tab_bulk = 0;
+  if constexpr (G::kFixed) {
+    if ((reinterpret_cast<uintptr_t>(P.a.lut.table) & 15u) == 0) tab_bulk = P.a.lut.count & ~3;
+  }
   if (tid == 0) {
+    if constexpr (G::kFixed) {
+      if (tab_bulk > 0) {  // completes on stage 0's barrier together with plane i0-1
+        mbar_add_tx(&bars[0], 4u * (uint32_t)tab_bulk);
+        bulk_copy_g2s(smem + G::TAB + 1, P.a.lut.table, 4u * (uint32_t)tab_bulk, &bars[0]);
+      }
+    }
     const int first = min(S, nplanes);
     for (int u = 0; u < first; ++u) issue_plane<G::kSlab>(P, smem, bars, u, i0, i1, j0);
     sh.issued = first;
   }
-  QPlane<V> Q[NS][3];
-  float mraw[V];  // sponge-table values fetched one plane ahead (fixed geometry)
-#pragma unroll
-  for (int e = 0; e < V; ++e) mraw[e] = 0.0f;
   if constexpr (G::kFixed) {
-    if (P.pf_mask < 0 && active) {
-      const int32_t q0 = qterm(i0, N) + K.qj;
-#pragma unroll
-      for (int e = 0; e < V; ++e) mraw[e] = mask_fetch(P.a.lut, q0 + K.qk[e]);
+    // The sponge table's whole 16-byte groups came with plane i0-1 (stage 0);
+    // threads store the rest and the two guards.  The barrier before the
+    // march orders them before the first lookup.
+    float* tab = smem + G::TAB;
+    const int cnt = P.a.lut.count;
+    for (int t = tab_bulk + tid; t < cnt; t += blockDim.x) tab[1 + t] = __ldg(P.a.lut.table + t);
+    if (tid == 0) {
+      tab[0] = 0.0f;
+      tab[cnt + 1] = 1.0f;
     }
   }
+  QPlane<V> Q[NS][3];
   // planes i0-1 (u = 0, stage 0) and i0 (u = 1, stage 1): both first uses, parity 0
   bool ok = mbar_wait_bounded(&bars[0], 0u, kWaitLimitNs);
   ok = mbar_wait_bounded(&bars[1 % S], 0u, kWaitLimitNs) && ok;
@@ -923,19 +981,19 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     int c = 0;
     // With a fixed 3-stage geometry, unrolled position p of the loop always
     // has its centre plane in stage (p + 1) % 3 and the next in (p + 2) % 3.
-    constexpr bool F = G::kFixed;
+    constexpr bool F = G::kStages == 3;
     while (true) {
       if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2, G, F ? 1 : -1, F ? 2 : -1>(
                         P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                        ph_nxt, K, active, mraw))
+                        ph_nxt, K, active))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0, G, F ? 2 : -1, F ? 0 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                          ph_nxt, K, active, mraw))
+                          ph_nxt, K, active))
         break;
       if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1, G, F ? 0 : -1, F ? 1 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
-                          ph_nxt, K, active, mraw))
+                          ph_nxt, K, active))
         break;
       ++c;
     }
@@ -1210,24 +1268,33 @@ std::mutex KernelSlot<LEVEL, V, QUEUE, COMP>::mu;
 template <int LEVEL, int V, bool QUEUE, bool COMP>
 int KernelSlot<LEVEL, V, QUEUE, COMP>::granted = 0;
 
-// Compile-time tiles for the headline sizes (resident layout, 3 stages).
-template <int LEVEL, int V, int N, int TJ>
+// Compile-time tiles for the headline sizes (resident layout).
+template <int LEVEL, int V, int N, int TJ, int S>
 struct FixedSlot {
   static std::mutex mu;
   static int granted;
-  static auto fn() { return tma_queue_kernel<LEVEL, V, false, GeomCT<N, TJ, QFields<LEVEL>::ns>>; }
+  static auto fn() {
+    return tma_queue_kernel<LEVEL, V, false, GeomCT<N, TJ, QFields<LEVEL>::ns, S>>;
+  }
 };
-template <int LEVEL, int V, int N, int TJ>
-std::mutex FixedSlot<LEVEL, V, N, TJ>::mu;
-template <int LEVEL, int V, int N, int TJ>
-int FixedSlot<LEVEL, V, N, TJ>::granted = 0;
+template <int LEVEL, int V, int N, int TJ, int S>
+std::mutex FixedSlot<LEVEL, V, N, TJ, S>::mu;
+template <int LEVEL, int V, int N, int TJ, int S>
+int FixedSlot<LEVEL, V, N, TJ, S>::granted = 0;
 
 struct FixedTile {
-  int level, V, N, TJ;
+  int level, V, N, TJ, S;
 };
 constexpr FixedTile kFixedTiles[] = {
-    {LFM_REAL, 4, 512, 4}, {LFM_REAL, 4, 256, 8}, {LFM_COMPLEX, 2, 512, 2},
-    {LFM_COMPLEX, 2, 256, 4}, {LFM_REAL, 4, 128, 8}, {LFM_COMPLEX, 2, 128, 4}};
+    {LFM_REAL, 4, 512, 4, 3}, {LFM_REAL, 4, 256, 8, 3}, {LFM_COMPLEX, 2, 512, 2, 3},
+    {LFM_COMPLEX, 2, 256, 4, 3}, {LFM_REAL, 4, 128, 8, 3}, {LFM_COMPLEX, 2, 128, 4, 3}};
+
+// The stage count of the compile-time tile (level, V, N, TJ); 0 if none.
+constexpr int fixed_stages(int level, int V, int N, int TJ) {
+  for (const FixedTile& t : kFixedTiles)
+    if (t.level == level && t.V == V && t.N == N && t.TJ == TJ) return t.S;
+  return 0;
+}
 
 // The fixed tile for (level, V, N), if any.
 const FixedTile* fixed_tile(int level, int V, int N) {
@@ -1238,17 +1305,25 @@ const FixedTile* fixed_tile(int level, int V, int N) {
 
 template <int LEVEL, int V, int N, int TJ>
 cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  using Slot = FixedSlot<LEVEL, V, N, TJ>;
+  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ)>;
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
 
+// Shared memory of the sponge table of the compile-time tiles: count entries
+// between a 0 and a 1, after 3 floats of padding that put the first entry on a
+// 16-byte boundary, rounded up to 16 bytes.
+int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
+
 // Launches the compile-time variant when the chosen tile is one of
-// kFixedTiles (3 stages, no streamed mask or S_a); false if there is none.
+// kFixedTiles (no streamed mask or S_a) and its ring plus the sponge table fit
+// in shared memory (ch.smem includes the table then); false if not.
 template <int LEVEL, int V>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
-  if (ch.S != 3 || P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
+  if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
   const FixedTile* t = fixed_tile(LEVEL, V, P.N);
-  if (!t || t->TJ != ch.TJ) return false;
+  if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
+  if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
+    return false;
   if constexpr (LEVEL == LFM_REAL && V == 4) {
     if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 4>(P, ch, stream); return true; }
     if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 8>(P, ch, stream); return true; }
@@ -1269,23 +1344,28 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   if (e != cudaSuccess) return e;
   // threads per CTA the register file can hold (at least one CTA per SM)
   const int max_threads = std::min(512, (65536 / std::max(regs, 1)) / 32 * 32);
-  // The mask table is read through L1: keep the shared-memory carveout small
-  // enough to leave L1 room for it (measured: staging it in shared memory
-  // instead is slower, bank conflicts of the random-key loads).
+  // The run-time geometry reads the mask table through L1: keep the
+  // shared-memory carveout small enough to leave L1 room for it.
   const int count = (P.pf_mask >= 0) ? 0 : P.a.lut.count;
   const int table_bytes = 4 * count;
   // Without a forced tile, the sizes with a compile-time variant take its
-  // tile (TJ rows, 3 stages); the planner still picks the plane chunk.
+  // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
+  // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
   const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns &&
                          !P.a.slab)
                             ? fixed_tile(LEVEL, V, P.N) : nullptr;
+  const int tab_smem = ft ? sponge_table_bytes(count) : 0;
+  if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {
-    fixed_cfg = TileConfig{ft->TJ, 3, 0, 0, 0, V};
+    fixed_cfg = TileConfig{ft->TJ, ft->S, 0, 0, 0, V};
     forced = &fixed_cfg;
   }
-  const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0,
-                           table_bytes, P.a.slab ? P.a.i_hi - P.a.i_lo : P.N);
+  // With a compile-time variant in reach the table sits in shared memory
+  // (extra_smem); otherwise it is read through L1.
+  const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced,
+                           ft ? tab_smem : 0, ft ? 0 : table_bytes,
+                           P.a.slab ? P.a.i_hi - P.a.i_lo : P.N);
   if (!ch.TJ) return cudaErrorNotSupported;
   P.TJ = ch.TJ;
   P.S = ch.S;

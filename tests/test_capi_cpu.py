@@ -136,6 +136,54 @@ def test_mask_table_edge_cases(lib):
     assert (one.lookup(radial_keys(N)) == 1).all()
 
 
+def _clamped_key_mask(N: int, desc, table: np.ndarray) -> np.ndarray:
+    """The compile-time step kernels' sponge lookup, in int32 as the kernel
+    computes it (csrc/step_tma.cu: key8, sponge_key, min_relu): a table
+    [0, table..., 1] indexed by a byte offset clamped to [0, 4 * (count + 1)]."""
+    i32 = np.int32
+    x = np.arange(N, dtype=i32)
+    key8 = (((2 * x - N + 1) ** 2) - 1) >> 3  # qterm is an odd square: 1 mod 8
+    key_lo = (i32(desc.q_lo) - i32(3)) >> 3
+    aj4 = (4 * (key8 + 1 - key_lo)).astype(i32)
+    cap4 = i32(4 * (desc.count + 1))
+    with np.errstate(over="raise"):
+        off = (4 * key8)[:, None, None] + aj4[None, :, None] + (4 * key8)[None, None, :]
+    assert off.dtype == np.int32
+    off = np.maximum(np.minimum(off, cap4), 0)
+    tab = np.concatenate([[0.0], table[: desc.count], [1.0]]).astype(np.float32)
+    return tab[off >> 2].ravel()
+
+
+@pytest.mark.parametrize("N", [8, 16, 36, 64])
+@pytest.mark.parametrize("bf", [0.1, 0.3, 0.7])
+def test_clamped_key_lookup_reproduces_the_mask(lib, N, bf):
+    from lfm_b200.mask import MaskTable, boundary_mask
+
+    m = boundary_mask(N, bf)
+    t = MaskTable.from_mask(N, m)
+    assert np.array_equal(_clamped_key_mask(N, t.desc, t.table).view(np.uint32), m.view(np.uint32))
+    f = MaskTable.for_lattice(N, bf)
+    assert np.array_equal(_clamped_key_mask(N, f.desc, f.table).view(np.uint32), m.view(np.uint32))
+
+
+def test_clamped_key_lookup_empty_bands_and_range(lib):
+    from lfm_b200.mask import MaskTable, boundary_mask
+
+    N = 12
+    for fill in (0.0, 1.0):
+        t = MaskTable.from_mask(N, np.full(N**3, fill, np.float32))
+        assert (_clamped_key_mask(N, t.desc, t.table) == fill).all()
+    # offsets stay inside int32 at the largest lattice, all-zero band included
+    i32 = np.iinfo(np.int32)
+    for N in (512, 2048):
+        key_max = 3 * ((N - 1) ** 2 - 1) // 8
+        for q_lo in (i32.max, 3, 0):
+            key_lo = (q_lo - 3) >> 3
+            lo, hi = 4 * (1 - key_lo), 4 * (key_max + 1 - key_lo)
+            assert i32.min <= lo and hi <= i32.max
+    del boundary_mask
+
+
 def test_bad_sizes_are_rejected(lib):
     import ctypes
 
