@@ -27,12 +27,12 @@ __device__ __forceinline__ RealOutT<T> real_cell_ab(T lapE, T e, T e_prev, T lap
   const T chi_sq = fmul(chi, chi);
   const T E_new = gov01(e, e_prev, lapE, chi_sq, s);
   // chi_source = (kappa/chi0)*chi*(E*E - e0_sq)
-  const T src = fmul(fmul(cst<T>(s.k_over_chi0), chi), fsub(fmul(e, e), cst<T>(s.e0_sq)));
+  const T src = fmul(pmul(cst<T>(s.k_over_chi0), chi), fsub(fmul(e, e), cst<T>(s.e0_sq)));
   T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
   RealOutT<T> o;
-  o.psi = fmul(E_new, absorb);
-  o.psi_prev = fmul(e, absorb);
+  o.psi = pmul(E_new, absorb);  // stored
+  o.psi_prev = pmul(e, absorb);
   o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
   o.chi_prev = chi;
   return o;
@@ -72,7 +72,7 @@ __device__ __forceinline__ T momentum_current(T pr, T pi, const FacesT<T>& R,
   const T jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
   const T jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
   const T jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
-  return fmul(cst<T>(0.5f), fadd(fadd(jx, jy), jz));  // j_total = 0.5*(j_x + j_y + j_z)
+  return pmul(cst<T>(0.5f), fadd(fadd(jx, jy), jz));  // j_total = 0.5*(j_x + j_y + j_z)
 }
 
 template <class T>
@@ -87,15 +87,15 @@ __device__ __forceinline__ ComplexOutT<T> complex_cell_ab(T lapR, T pr, T pr_pre
   const T psi_sq = fadd(fmul(pr, pr), fmul(pi, pi));
   const T jt = momentum_current(pr, pi, R, I);
   // (kappa/chi0)*chi*(psi_sq + eps_w*j - e0_sq)
-  const T src = fmul(fmul(cst<T>(s.k_over_chi0), chi),
+  const T src = fmul(pmul(cst<T>(s.k_over_chi0), chi),
                      fsub(fadd(psi_sq, fmul(cst<T>(s.eps_w), jt)), cst<T>(s.e0_sq)));
   T acc = fsub(lapX, src);
   acc = mexican_hat(acc, chi, chi_sq, s);
   ComplexOutT<T> o;
-  o.pr = fmul(Pr_new, absorb);
-  o.pi = fmul(Pi_new, absorb);
-  o.pr_prev = fmul(pr, absorb);
-  o.pi_prev = fmul(pi, absorb);
+  o.pr = pmul(Pr_new, absorb);  // stored
+  o.pi = pmul(Pi_new, absorb);
+  o.pr_prev = pmul(pr, absorb);
+  o.pi_prev = pmul(pi, absorb);
   o.chi = gov02_finish(chi, chi_prev, acc, mask, absorb, s);
   o.chi_prev = chi;
   return o;

@@ -60,6 +60,20 @@ __device__ __forceinline__ F2 fsub(F2 a, F2 b) {
   return d;
 }
 
+// A product whose every consumer is a multiplication or a store, never an
+// addition: then nothing can contract it, and two cells take one packed
+// FMUL2.  (fmul above stays scalar because its products do feed additions.)
+__device__ __forceinline__ float pmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ F2 pmul(F2 a, F2 b) {
+  unsigned long long ra, rb, rd;
+  memcpy(&ra, &a.v, 8);
+  memcpy(&rb, &b.v, 8);
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(rd) : "l"(ra), "l"(rb));
+  F2 d;
+  memcpy(&d.v, &rd, 8);
+  return d;
+}
+
 // A float constant as the value type T (broadcast to both lanes for F2).
 template <class T>
 __device__ __forceinline__ T cst(float a);
@@ -68,10 +82,16 @@ __device__ __forceinline__ float cst<float>(float a) { return a; }
 template <>
 __device__ __forceinline__ F2 cst<F2>(float a) { return pk(a, a); }
 
-// x < lo ? lo : x per lane (a NaN stays NaN, as NumPy's boolean-mask clamp keeps it)
-__device__ __forceinline__ float clamp_below(float x, float lo) { return x < lo ? lo : x; }
+// x < lo ? lo : x per lane (a NaN stays NaN, as NumPy's boolean-mask clamp
+// keeps it), as one max.NaN: for a number lo it returns lo below lo, x from
+// lo up, and NaN for a NaN x.
+__device__ __forceinline__ float clamp_below(float x, float lo) {
+  float d;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(x), "f"(lo));
+  return d;
+}
 __device__ __forceinline__ F2 clamp_below(F2 x, float lo) {
-  return pk(x.v.x < lo ? lo : x.v.x, x.v.y < lo ? lo : x.v.y);
+  return pk(clamp_below(x.v.x, lo), clamp_below(x.v.y, lo));
 }
 
 // Scalar parameters rounded to float32 on the host the way NumPy rounds a

@@ -682,7 +682,9 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   const int s_nxt = SNXT >= 0 ? SNXT : s_nxt_rt;
   // packed two-cell arithmetic in the compile-time tiles (V even)
   constexpr bool PK = (V % 2 == 0);
-  if (*(volatile int*)&sh.abort_flag) return false;
+  // another warp gave up on a wait: stop (looked at once per unrolled round
+  // of three planes; a plane's own wait is bounded anyway)
+  if (PA == 0 && *(volatile int*)&sh.abort_flag) return false;
   if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
     *(volatile int*)&sh.abort_flag = 1;
     atomicOr(a.status, LFM_ERR_DEVICE_TIMEOUT);
