@@ -943,6 +943,7 @@ struct BatchPlan {
   std::vector<lfm::BatchItem> items;  // REAL items, then COMPLEX, each largest first
   int real_items = 0;
   int threads = 0, smem = 0, grid = 0;
+  int tab_off = -1;  // float offset of the shared-memory sponge table, -1 = through L1
   std::vector<int> TJ, IC, stage_floats;
 };
 
@@ -1027,6 +1028,17 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
   for (const lfm::BatchItem& it : plan->items) plan->real_items += it.level == LFM_REAL;
   plan->threads = threads;
   plan->smem = t.stages * max_stage * (int)sizeof(float);
+  // The sponge tables (one lattice's at a time) after the largest ring, when
+  // the largest of them fits; tab[1] lands on a 16-byte boundary (stage
+  // floats are multiples of N, N of 4).
+  int tab_bytes = 0;
+  for (int l = 0; l < count; ++l)
+    tab_bytes = std::max(tab_bytes, (4 * (L[l].lut.count + 5) + 15) / 16 * 16);
+  plan->tab_off = -1;
+  if (plan->smem + tab_bytes <= kBatchSmemLimit) {
+    plan->tab_off = t.stages * max_stage + 3;
+    plan->smem += tab_bytes;
+  }
   if (plan->smem > kBatchSmemLimit)
     return fail(LFM_ERR_UNSUPPORTED, "batch needs %d B of shared memory per CTA (limit %d)",
                 plan->smem, kBatchSmemLimit);
@@ -1043,6 +1055,7 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
 struct lfm_batch {
   int device = 0;
   int stages = 3;
+  int tab_off = -1;
   lfm::BatchLattice* d_lat = nullptr;
   lfm::BatchItem* d_items = nullptr;
   int* d_counters = nullptr;  // next REAL item, next COMPLEX item, retired CTAs
@@ -1139,6 +1152,7 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
   lfm_batch* B = new lfm_batch;
   B->device = device;
   B->stages = t.stages;
+  B->tab_off = plan.tab_off;
   B->nitems = (int)plan.items.size();
   B->real_items = plan.real_items;
   B->threads = plan.threads;
@@ -1177,6 +1191,7 @@ int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
   P.parity = parity;
   P.damp_prev = damp_prev ? 1 : 0;
   P.stages = batch->stages;
+  P.tab_off = batch->tab_off;
   P.status = status;
   P.next_item = batch->d_counters;
   P.retired = batch->d_counters + 2;

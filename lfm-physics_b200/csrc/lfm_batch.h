@@ -37,6 +37,7 @@ struct BatchParams {
   int parity;     // slot holding the current fields
   int damp_prev;  // previous-field slots hold undamped values
   int stages;
+  int tab_off;     // float offset of the shared-memory sponge table, -1 = read through L1
   int* status;
   int* next_item;  // work-list counters (REAL, COMPLEX), 0 between launches
   int* retired;    // CTAs that took their last item, 0 between launches

@@ -49,6 +49,7 @@ struct TmaParams {
   int pf_sa;                     // index of S_a colour 0, -1 = none
   int N, TJ, IC, S, JT;
   int stage_floats;
+  int tab_off;  // float offset of the shared-memory sponge table's tab[0], -1 = read through L1
 };
 
 // ---- PTX helpers -------------------------------------------------------------
@@ -124,12 +125,35 @@ __device__ __forceinline__ uint64_t now_ns() {
   return t;
 }
 
+// try_wait that may suspend the thread for up to hint_ns until the phase
+// completes (it resumes as soon as it does), so a waiting warp sleeps instead
+// of spinning on the issue slots of the warps that have their data.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity,
+                                                    uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr uint32_t kSleepHintNs = 2000;
+
+// SLEEP: retry with mbar_try_wait_sleep.  Measured on the long single-lattice
+// marches: +0.4-0.8% (300 ns to 20 us alike); on the batch kernel's short
+// items: -5.6%, so there the retries spin.
+template <bool SLEEP = false>
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
                                                   uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = now_ns();
   while (true) {
-    if (mbar_try_wait(bar, parity)) return true;
+    if (SLEEP ? mbar_try_wait_sleep(bar, parity, kSleepHintNs) : mbar_try_wait(bar, parity))
+      return true;
     if (now_ns() - t0 > limit_ns) return false;
   }
 }
@@ -515,21 +539,20 @@ struct QLane {
   int o_pt;                                // point rows at k0 (from the stage base)
 };
 
-// Radial keys of a thread's cells: q = qterm(i) + qj + qk[e].  The
-// compile-time tiles use byte offsets into the shared-memory sponge table
-// instead: offset = min_relu(4*key8(i) + aj4 + ak4[e], cap4) (see sponge_key).
+// Radial keys of a thread's cells.  A cell's key q = qterm(i) + qterm(j) +
+// qterm(k0 + e) is 3 mod 8 for even N (each term an odd square, 1 mod 8) and
+// 0 mod 4 for odd N (even squares); the table steps by 2^shift, shift 3 or 2.
+// Then q >> shift = (qterm(i) >> shift) + (qterm(j) >> shift) +
+// (qterm(k) >> shift) exactly, so a table offset is a sum of three per-axis
+// terms: offset = min_relu(4*(qterm(i) >> shift) + aj4 + ak4[e], cap4).
 template <int V>
 struct QKeys {
-  int32_t qj;
-  int32_t qk[V];
+  int32_t qj;  // qterm(j)
   int32_t aj4, cap4;
-  int32_t ak4[V];
+  int32_t ak4[V];  // 4 * (qterm(k0 + e) >> shift)
 };
 
-// (qterm(x, N) - 1) / 8 for even N.  qterm is an odd square, 1 mod 8, so a
-// cell's key q = 8 * (key8(i) + key8(j) + key8(k)) + 3 exactly, and q >> 3 is
-// the sum of the three.
-__device__ __forceinline__ int32_t key8(int x, int N) { return (qterm(x, N) - 1) >> 3; }
+__device__ __forceinline__ int key_shift(int N) { return (N & 1) ? 2 : 3; }
 
 // max(min(a, b), 0) in one instruction.
 __device__ __forceinline__ int32_t min_relu(int32_t a, int32_t b) {
@@ -538,34 +561,49 @@ __device__ __forceinline__ int32_t min_relu(int32_t a, int32_t b) {
   return d;
 }
 
-// The sponge table in shared memory, for the compile-time tiles:
+// The sponge table in shared memory:
 //   tab[0] = 0, tab[1 + t] = lut.table[t] (t < count), tab[count + 1] = 1,
 // with tab[1] on a 16-byte boundary so the copy engine can fill it.
-// A cell's entry is t = q/8 - q_lo/8 + 1 clamped to [0, count + 1]: keys below
-// the band land on the 0, keys above it on the 1, so the lookup needs no band
-// test and no select.  (q_lo - 3) >> 3 also covers the two empty bands: the
-// all-zero mask (q_lo = INT32_MAX, every offset clamps to 0) and the all-one
-// mask (q_lo = 0, count = 0, every offset clamps to 1).
+// A cell's entry is t = (q >> shift) - (q_lo >> shift) + 1 clamped to
+// [0, count + 1]: keys below the band land on the 0, keys above it on the 1,
+// so the lookup needs no band test and no select.  q_lo is capped at 3 N^2
+// (above every key) for the all-zero mask (q_lo = INT32_MAX): every offset
+// clamps to 0 then; the all-one mask (q_lo = 0, count = 0) clamps to 1.
 template <int V>
 __device__ __forceinline__ void sponge_key(QKeys<V>& K, const MaskLut& lut, int j, int k0,
                                            int N) {
-  const int32_t key_lo = (lut.q_lo - 3) >> 3;
-  K.aj4 = 4 * (key8(j, N) + 1 - key_lo);
+  const int sh = key_shift(N);
+  const int32_t key_lo = min(lut.q_lo, 3 * N * N) >> sh;
+  K.qj = qterm(j, N);
+  K.aj4 = 4 * ((K.qj >> sh) + 1 - key_lo);
   K.cap4 = 4 * (lut.count + 1);
 #pragma unroll
-  for (int e = 0; e < V; ++e) K.ak4[e] = 4 * key8(k0 + e, N);
+  for (int e = 0; e < V; ++e) K.ak4[e] = 4 * (qterm(k0 + e, N) >> sh);
 }
 
-// Mask values of a thread's cells.  The table load is predicated on the band
-// test (mask_from_q_flat): a branch around whole rows inside or beyond the
-// sponge was measured slower (143.8 -> 134.3 GCell/s at 512^3 REAL), as it
-// keeps the compiler from hoisting the loads.
+// Mask values of a thread's cells from the shared-memory table (sponge_key).
 template <int V>
-__device__ __forceinline__ void q_mask(const MaskLut& lut, int32_t qi, const QKeys<V>& K,
+__device__ __forceinline__ void tab_mask(const float* tab, int32_t qi, int N, const QKeys<V>& K,
+                                         float (&mask)[V]) {
+  const int32_t b4 = 4 * (qi >> key_shift(N)) + K.aj4;
+  const char* t = reinterpret_cast<const char*>(tab);
+#pragma unroll
+  for (int e = 0; e < V; ++e)
+    mask[e] = *reinterpret_cast<const float*>(t + min_relu(b4 + K.ak4[e], K.cap4));
+}
+
+// Mask values through L1 from the global table, for lattices whose table does
+// not fit beside the ring.  The table load is predicated on the band test
+// (mask_from_q_flat); qterm(k) comes back from ak4: 2 * ak4 + 1 for even N
+// (8a + 1 = 2 * 4a + 1), ak4 itself for odd N (4b).
+template <int V>
+__device__ __forceinline__ void q_mask(const MaskLut& lut, int32_t qi, int N, const QKeys<V>& K,
                                        float (&mask)[V]) {
   const int32_t qij = qi + K.qj;
+  const bool even = !(N & 1);
 #pragma unroll
-  for (int e = 0; e < V; ++e) mask[e] = mask_from_q_flat(lut, qij + K.qk[e]);
+  for (int e = 0; e < V; ++e)
+    mask[e] = mask_from_q_flat(lut, qij + (even ? 2 * K.ak4[e] + 1 : K.ak4[e]));
 }
 
 template <int V>
@@ -627,14 +665,20 @@ struct QFields {
 // lattice, any tile); GeomCT<N, TJ, NS> fixes it at compile time for the
 // headline tiles (3 stages, resident point fields), so every shared-memory
 // offset of a plane folds into an immediate beside one per-thread base.
-struct GeomRT {
+// TABM: where the sponge table is read: 0 = as P.tab_off says at run time,
+// 1 = shared memory (P.tab_off), -1 = through L1.
+template <int TABM>
+struct GeomRTT {
   static constexpr bool kFixed = false;
   static constexpr bool kSlab = true;  // may step a slab (plane range, ghost planes)
   static constexpr int kStages = 0;    // stage count known at run time only
+  static constexpr int TAB = -1;       // the sponge table's place comes with the parameters
+  static constexpr int kTabMode = TABM;
   int N, TJ, S, SF;
-  __device__ __forceinline__ explicit GeomRT(const TmaParams& P)
+  __device__ __forceinline__ explicit GeomRTT(const TmaParams& P)
       : N(P.N), TJ(P.TJ), S(P.S), SF(P.stage_floats) {}
 };
+using GeomRT = GeomRTT<0>;
 
 template <int N_, int TJ_, int NS_, int S_ = 3>
 struct GeomCT {
@@ -644,6 +688,7 @@ struct GeomCT {
   static constexpr int kStages = S_;
   static constexpr int N = N_, TJ = TJ_, S = S_, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
   static constexpr int TAB = S * SF + 3;  // float offset of the sponge table's tab[0]
+  static constexpr int kTabMode = 1;
   __device__ __forceinline__ explicit GeomCT(const TmaParams&) {}
 };
 
@@ -685,7 +730,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   // another warp gave up on a wait: stop (looked at once per unrolled round
   // of three planes; a plane's own wait is bounded anyway)
   if (PA == 0 && *(volatile int*)&sh.abort_flag) return false;
-  if (!mbar_wait_bounded(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
+  if (!mbar_wait_bounded<G::kFixed>(&bars[s_nxt], ph_nxt, kWaitLimitNs)) {
     *(volatile int*)&sh.abort_flag = 1;
     atomicOr(a.status, LFM_ERR_DEVICE_TIMEOUT);
     return false;
@@ -702,19 +747,19 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   const int i = i0 + c;
   const int j = L.j, k0 = L.k0;
   float mask[V], absorb[V];
-  if (P.pf_mask >= 0) {
+  if constexpr (G::kFixed) {
+    // the compile-time tiles never stream the mask; their table sits at TAB
+    tab_mask<V>(smem + G::TAB, qterm(i, N), N, K, mask);
+  } else if (P.pf_mask >= 0) {  // the streamed mask, from the centre plane's stage
     const Vec<V> m = lds<V>(smem, bc + L.o_pt + P.pf_mask * PTS);
 #pragma unroll
     for (int e = 0; e < V; ++e) mask[e] = m.v[e];
-  } else if constexpr (G::kFixed) {
-    // the shared-memory table with its clamped key (sponge_key)
-    const int32_t b4 = 4 * key8(i, N) + K.aj4;
-    const char* tab = reinterpret_cast<const char*>(smem + G::TAB);
-#pragma unroll
-    for (int e = 0; e < V; ++e)
-      mask[e] = *reinterpret_cast<const float*>(tab + min_relu(b4 + K.ak4[e], K.cap4));
   } else {
-    q_mask<V>(a.lut, qterm(i + (G::kSlab ? a.i_off : 0), N), K, mask);
+    const int32_t qi = qterm(i + (G::kSlab ? a.i_off : 0), N);  // a slab's global plane
+    if (G::kTabMode > 0 || (G::kTabMode == 0 && P.tab_off >= 0))
+      tab_mask<V>(smem + P.tab_off, qi, N, K, mask);
+    else
+      q_mask<V>(a.lut, qi, N, K, mask);
   }
 #pragma unroll
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
@@ -911,10 +956,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   L.o_pr = (r + 2) * N + kpv;
   L.o_pt = NS * (TJ + 2) * N + r * N + k0;
   QKeys<V> K;
-  K.qj = qterm(j0 + r, N);
-#pragma unroll
-  for (int e = 0; e < V; ++e) K.qk[e] = qterm(k0 + e, N);
-  if constexpr (G::kFixed) sponge_key<V>(K, P.a.lut, j0 + r, k0, N);
+  sponge_key<V>(K, P.a.lut, j0 + r, k0, N);
 
   __syncthreads();  // a previous march in this CTA is over in every warp
   if (tid == 0) {
@@ -927,28 +969,28 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     mbar_init_fence();
   }
   __syncthreads();
-  // floats of the sponge table the copy engine moves (compile-time tiles):
-  // whole 16-byte groups of a 16-byte aligned table
+  // The sponge table in shared memory (tab_at = offset of tab[0], < 0 when it
+  // is read through L1): the copy engine moves the whole 16-byte groups of a
+  // 16-byte aligned table, completing on stage 0's barrier together with
+  // plane i0-1; threads store the rest and the two guards.  The barrier
+  // before the march orders them before the first lookup.
+  const int tab_at = G::kFixed ? G::TAB : (G::kTabMode < 0 ? -1 : P.tab_off);
   int tab_bulk = 0;
-  if constexpr (G::kFixed) {
-    if ((reinterpret_cast<uintptr_t>(P.a.lut.table) & 15u) == 0) tab_bulk = P.a.lut.count & ~3;
-  }
+  if (tab_at >= 0 && (reinterpret_cast<uintptr_t>(P.a.lut.table) & 15u) == 0)
+    tab_bulk = P.a.lut.count & ~3;
   if (tid == 0) {
-    if constexpr (G::kFixed) {
-      if (tab_bulk > 0) {  // completes on stage 0's barrier together with plane i0-1
-        mbar_add_tx(&bars[0], 4u * (uint32_t)tab_bulk);
-        bulk_copy_g2s(smem + G::TAB + 1, P.a.lut.table, 4u * (uint32_t)tab_bulk, &bars[0]);
-      }
+    // a previous march of this CTA read this shared memory (generic proxy)
+    fence_proxy_async_smem();
+    if (tab_bulk > 0) {
+      mbar_add_tx(&bars[0], 4u * (uint32_t)tab_bulk);
+      bulk_copy_g2s(smem + tab_at + 1, P.a.lut.table, 4u * (uint32_t)tab_bulk, &bars[0]);
     }
     const int first = min(S, nplanes);
     for (int u = 0; u < first; ++u) issue_plane<G::kSlab>(P, smem, bars, u, i0, i1, j0);
     sh.issued = first;
   }
-  if constexpr (G::kFixed) {
-    // The sponge table's whole 16-byte groups came with plane i0-1 (stage 0);
-    // threads store the rest and the two guards.  The barrier before the
-    // march orders them before the first lookup.
-    float* tab = smem + G::TAB;
+  if (tab_at >= 0) {
+    float* tab = smem + tab_at;
     const int cnt = P.a.lut.count;
     for (int t = tab_bulk + tid; t < cnt; t += blockDim.x) tab[1 + t] = __ldg(P.a.lut.table + t);
     if (tid == 0) {
@@ -1073,10 +1115,11 @@ __device__ __forceinline__ void batch_params(TmaParams& P, const BatchLattice& L
   P.S = B.stages;
   P.JT = L.N / L.TJ;
   P.stage_floats = L.stage_floats;
+  P.tab_off = B.tab_off;  // after the largest ring of the batch, or -1
 }
 
 // The item loop of one level: CTAs take items through that level's counter.
-template <int LEVEL, int V>
+template <int LEVEL, int V, int TABM>
 __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchItem* items,
                                             int nitems, int* next_item, float* smem,
                                             uint64_t* bars, QShared& sh, TmaParams& P,
@@ -1090,7 +1133,7 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
     const BatchItem it = items[w];
     if (threadIdx.x == 0) batch_params<LEVEL>(P, B.lattices[it.lattice], B);
     __syncthreads();  // P is visible to every thread
-    q_march<LEVEL, V, false, true>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
+    q_march<LEVEL, V, false, true, GeomRTT<TABM>>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
     __syncthreads();  // every wait of the march is over
     if (sh.abort_flag) break;  // same value in every thread
     if (threadIdx.x == 0)
@@ -1101,7 +1144,9 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
 // Every CTA drains the REAL list, then the COMPLEX list: a CTA done with
 // the REAL items starts on the COMPLEX ones at once, so the launch has a
 // single tail (the smallest COMPLEX items).  The two loops run one after the
-// other, so their register demands do not add up.
+// other, so their register demands do not add up.  TABM: the sponge tables in
+// shared memory (1, B.tab_off >= 0) or through L1 (-1).
+template <int TABM>
 __global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ BatchParams B) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
@@ -1110,10 +1155,10 @@ __global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ 
   __shared__ int s_item;
   sh.abort_flag = 0;
   if (B.real_items > 0)
-    batch_level<LFM_REAL, 4>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P, s_item);
+    batch_level<LFM_REAL, 4, TABM>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P, s_item);
   __syncthreads();
   if (!sh.abort_flag && B.nitems > B.real_items)
-    batch_level<LFM_COMPLEX, 2>(B, B.items + B.real_items, B.nitems - B.real_items,
+    batch_level<LFM_COMPLEX, 2, TABM>(B, B.items + B.real_items, B.nitems - B.real_items,
                                 B.next_item + 1, smem, bars, sh, P, s_item);
   if (threadIdx.x == 0) {
     __threadfence();
@@ -1346,10 +1391,13 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   if (e != cudaSuccess) return e;
   // threads per CTA the register file can hold (at least one CTA per SM)
   const int max_threads = std::min(512, (65536 / std::max(regs, 1)) / 32 * 32);
-  // The run-time geometry reads the mask table through L1: keep the
-  // shared-memory carveout small enough to leave L1 room for it.
+  // The register-queue kernels keep the sponge table in shared memory after
+  // the ring when it fits (tab_smem); otherwise they read it through L1, and
+  // the carveout must leave L1 room for it (table_bytes).
   const int count = (P.pf_mask >= 0) ? 0 : P.a.lut.count;
   const int table_bytes = 4 * count;
+  const bool want_tab = QUEUE && P.pf_mask < 0;
+  const int tab_smem = want_tab ? sponge_table_bytes(count) : 0;
   // Without a forced tile, the sizes with a compile-time variant take its
   // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
   // memory; the planner still picks the plane chunk.
@@ -1357,23 +1405,28 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns &&
                          !P.a.slab)
                             ? fixed_tile(LEVEL, V, P.N) : nullptr;
-  const int tab_smem = ft ? sponge_table_bytes(count) : 0;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {
     fixed_cfg = TileConfig{ft->TJ, ft->S, 0, 0, 0, V};
     forced = &fixed_cfg;
   }
-  // With a compile-time variant in reach the table sits in shared memory
-  // (extra_smem); otherwise it is read through L1.
-  const Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced,
-                           ft ? tab_smem : 0, ft ? 0 : table_bytes,
-                           P.a.slab ? P.a.i_hi - P.a.i_lo : P.N);
+  const int planes = P.a.slab ? P.a.i_hi - P.a.i_lo : P.N;
+  bool tab_in_smem = want_tab;
+  Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, tab_smem, 0,
+                     planes);
+  if (!ch.TJ && want_tab) {  // the table does not fit beside any ring: through L1
+    tab_in_smem = false;
+    ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0, table_bytes,
+                planes);
+  }
   if (!ch.TJ) return cudaErrorNotSupported;
   P.TJ = ch.TJ;
   P.S = ch.S;
   P.IC = ch.IC;
   P.JT = P.N / ch.TJ;
   P.stage_floats = stage_bytes(P.N, ch.TJ, P.ns, P.np) / 4;
+  // tab[1] lands on a 16-byte boundary: stage_floats is a multiple of N, N of 4
+  P.tab_off = tab_in_smem ? ch.S * P.stage_floats + 3 : -1;
   TileConfig used{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem, V};
   tune_record(LEVEL, P.N, used);
   if constexpr (QUEUE && !COMP) {
@@ -1394,6 +1447,7 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   P.a = a;
   P.N = N;
   P.pf_mask = -1;
+  P.tab_off = -1;  // set by the planner when the table goes to shared memory
   P.pf_sa = -1;
   const int64_t n3 = (int64_t)N * N * N;
   if (a.level == LFM_REAL) {
@@ -1465,7 +1519,7 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
 // ---- batch launcher -------------------------------------------------------------
 namespace {
 std::mutex g_batch_mu;
-int g_batch_granted = 0;  // dynamic shared memory granted to the batch kernel
+int g_batch_granted[2] = {0, 0};  // dynamic shared memory granted to the two batch kernels
 
 template <typename K>
 cudaError_t grant_smem(K kernel, int smem, int* granted) {
@@ -1485,18 +1539,22 @@ cudaError_t grant_smem(K kernel, int smem, int* granted) {
 }  // namespace
 
 cudaError_t batch_kernel_regs(int* regs) {
-  cudaFuncAttributes fa{};
-  cudaError_t e = cudaFuncGetAttributes(&fa, tma_batch_kernel);
-  if (e == cudaSuccess) *regs = fa.numRegs;
+  // the larger of the two variants' demands
+  cudaFuncAttributes fa{}, fb{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, tma_batch_kernel<1>);
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fb, tma_batch_kernel<-1>);
+  if (e == cudaSuccess) *regs = std::max(fa.numRegs, fb.numRegs);
   return e;
 }
 
 cudaError_t launch_batch_step(const BatchParams& B, int threads, int smem, int grid,
                               cudaStream_t stream) {
   if (B.nitems == 0) return cudaSuccess;
-  cudaError_t e = grant_smem(tma_batch_kernel, smem, &g_batch_granted);
+  const bool tab = B.tab_off >= 0;
+  auto kernel = tab ? tma_batch_kernel<1> : tma_batch_kernel<-1>;
+  cudaError_t e = grant_smem(kernel, smem, &g_batch_granted[tab ? 1 : 0]);
   if (e != cudaSuccess) return e;
-  tma_batch_kernel<<<grid, threads, smem, stream>>>(B);
+  kernel<<<grid, threads, smem, stream>>>(B);
   return cudaGetLastError();
 }
 

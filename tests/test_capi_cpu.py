@@ -137,24 +137,26 @@ def test_mask_table_edge_cases(lib):
 
 
 def _clamped_key_mask(N: int, desc, table: np.ndarray) -> np.ndarray:
-    """The compile-time step kernels' sponge lookup, in int32 as the kernel
-    computes it (csrc/step_tma.cu: key8, sponge_key, min_relu): a table
-    [0, table..., 1] indexed by a byte offset clamped to [0, 4 * (count + 1)]."""
+    """The step kernels' shared-memory sponge lookup, in int32 as the kernel
+    computes it (csrc/step_tma.cu: key_shift, sponge_key, tab_mask, min_relu):
+    a table [0, table..., 1] indexed by a byte offset clamped to
+    [0, 4 * (count + 1)], the offset a sum of per-axis terms qterm >> shift."""
     i32 = np.int32
+    sh = 2 if N % 2 else 3
     x = np.arange(N, dtype=i32)
-    key8 = (((2 * x - N + 1) ** 2) - 1) >> 3  # qterm is an odd square: 1 mod 8
-    key_lo = (i32(desc.q_lo) - i32(3)) >> 3
-    aj4 = (4 * (key8 + 1 - key_lo)).astype(i32)
+    term4 = (4 * ((2 * x - N + 1) ** 2 >> sh)).astype(i32)
+    key_lo = i32(min(int(desc.q_lo), 3 * N * N) >> sh)
+    aj4 = (term4 + 4 * (1 - key_lo)).astype(i32)
     cap4 = i32(4 * (desc.count + 1))
     with np.errstate(over="raise"):
-        off = (4 * key8)[:, None, None] + aj4[None, :, None] + (4 * key8)[None, None, :]
+        off = term4[:, None, None] + aj4[None, :, None] + term4[None, None, :]
     assert off.dtype == np.int32
     off = np.maximum(np.minimum(off, cap4), 0)
     tab = np.concatenate([[0.0], table[: desc.count], [1.0]]).astype(np.float32)
     return tab[off >> 2].ravel()
 
 
-@pytest.mark.parametrize("N", [8, 16, 36, 64])
+@pytest.mark.parametrize("N", [8, 9, 16, 21, 36, 64])
 @pytest.mark.parametrize("bf", [0.1, 0.3, 0.7])
 def test_clamped_key_lookup_reproduces_the_mask(lib, N, bf):
     from lfm_b200.mask import MaskTable, boundary_mask
@@ -167,21 +169,21 @@ def test_clamped_key_lookup_reproduces_the_mask(lib, N, bf):
 
 
 def test_clamped_key_lookup_empty_bands_and_range(lib):
-    from lfm_b200.mask import MaskTable, boundary_mask
+    from lfm_b200.mask import MaskTable
 
-    N = 12
-    for fill in (0.0, 1.0):
-        t = MaskTable.from_mask(N, np.full(N**3, fill, np.float32))
-        assert (_clamped_key_mask(N, t.desc, t.table) == fill).all()
-    # offsets stay inside int32 at the largest lattice, all-zero band included
+    for N in (12, 13):
+        for fill in (0.0, 1.0):
+            t = MaskTable.from_mask(N, np.full(N**3, fill, np.float32))
+            assert (_clamped_key_mask(N, t.desc, t.table) == fill).all()
+    # offsets stay inside int32 up to the largest lattice (q_lo capped at 3 N^2)
     i32 = np.iinfo(np.int32)
-    for N in (512, 2048):
-        key_max = 3 * ((N - 1) ** 2 - 1) // 8
+    for N in (511, 512, 2047, 2048):
+        sh = 2 if N % 2 else 3
+        key_max = (3 * (N - 1) ** 2) >> sh
         for q_lo in (i32.max, 3, 0):
-            key_lo = (q_lo - 3) >> 3
+            key_lo = min(q_lo, 3 * N * N) >> sh
             lo, hi = 4 * (1 - key_lo), 4 * (key_max + 1 - key_lo)
             assert i32.min <= lo and hi <= i32.max
-    del boundary_mask
 
 
 def test_bad_sizes_are_rejected(lib):
