@@ -1215,7 +1215,10 @@ Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threa
       const int ctas = std::max(1, std::min(std::min(cta_by_smem, cta_by_thr), cta_by_reg));
       const double warps = std::min(ctas * threads / 32, 48);
       const double halo = (double)TJ / (TJ + 2);  // useful fraction of stencil rows
-      const double depth = std::min(S - (min_s - 1), 2) / 2.0;  // planes streamed ahead
+      // planes streamed ahead; the register-queue kernels measured no gain
+      // from a second plane in flight (3 vs 4 stages at 256^3 and 512^3), so
+      // their bonus stops at one and the smaller ring wins the tie
+      const double depth = std::min(S - (min_s - 1), queue ? 1 : 2) / 2.0;
       // L1 left beside the shared-memory carveout must hold the mask table
       const int l1_kb = 256 - carveout_kb(ctas * (smem + 1024));
       // (measured at 512^3: a 60-92 KB L1 beside the 67 KB table runs 10-15% slower)
