@@ -59,7 +59,8 @@ def parse():
     ap.add_argument("--level", choices=["real", "complex"], default="real",
                     help="level of the main leg; complex (with the packets as both parts) is a "
                          "secondary workload and turns the e2e, compensated and CPU legs off")
-    ap.add_argument("--batch-tuning", choices=["auto", "default"], default="auto")
+    ap.add_argument("--batch-tuning", default="auto",
+                    help="auto (the autotuner), default, or THREADS,STAGES,ITEM_CELLS")
     ap.add_argument("--adjoint-steps", type=int, default=500)
     return ap.parse_args()
 
@@ -284,10 +285,14 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
 
     os.environ.setdefault("LFM_B200_TUNE_CACHE", str(Path(tempfile.gettempdir()) /
                                                      "lfm_b200_bench_tune.json"))
-    B = BatchedLattices(cfgs, backend=be,
-                        tuning="auto" if args.batch_tuning == "auto" else None)
-    tune = B.tune_report or {"best": dict(threads=256, stages=3, item_cells=65536),
-                             "ms_per_step": None, "trials": []}
+    if args.batch_tuning in ("auto", "default"):
+        tuning = "auto" if args.batch_tuning == "auto" else None
+        fixed = dict(threads=256, stages=3, item_cells=65536)
+    else:
+        t, s_, c_ = (int(x) for x in args.batch_tuning.split(","))
+        tuning = fixed = dict(threads=t, stages=s_, item_cells=c_)
+    B = BatchedLattices(cfgs, backend=be, tuning=tuning)
+    tune = B.tune_report or {"best": fixed, "ms_per_step": None, "trials": []}
     B.graph_block = steps
     for i, (c, pr, pi) in enumerate(L):
         load(B, i, pr, pi)

@@ -978,8 +978,8 @@ int check_lattice_shape(const lfm_lattice_desc& d, int l) {
 
 // Bytes a cell moves per step (the sort key's weight): REAL 6 fields x 4 B,
 // COMPLEX 9.
-inline long item_cost(const lfm::BatchItem& it, int TJ, int N) {
-  return (long)TJ * N * (it.i1 - it.i0) * (it.level == LFM_REAL ? 24 : 36);
+inline long item_cost(const lfm::BatchItem& it, int N) {
+  return (long)(it.j1 - it.j0) * N * (it.i1 - it.i0) * (it.level == LFM_REAL ? 24 : 36);
 }
 
 // regs: registers per thread of the batch kernel; sms: SM count.
@@ -999,9 +999,15 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
     if (tpr > t.threads)
       return fail(LFM_ERR_UNSUPPORTED, "lattice %d: a row of N=%d needs %d threads > %d", l, N,
                   tpr, t.threads);
-    int TJ = 1;
-    for (int d = 1; d <= N; ++d)
-      if (N % d == 0 && d * tpr <= t.threads) TJ = d;
+    // As few row tiles as the CTA allows, their rows as even as possible
+    // (N / tiles or one more; they need not divide N), so that about all of
+    // the CTA's threads have cells (N = 96 REAL at 512 threads: 5 tiles of
+    // 20, 19, 19, 19, 19 rows and 90 % of the lanes, against 6 x 16 rows and
+    // 75 % with a divisor of N).  TJ is the largest tile.
+    const int tj_max = t.threads / tpr;
+    const int tiles = (N + tj_max - 1) / tj_max;
+    const int base = N / tiles, rem = N % tiles;
+    const int TJ = base + (rem > 0 ? 1 : 0);
     // chunks of about item_cells cells, the planes split as evenly as possible
     const double cells = (double)TJ * N * N;
     const int chunks = std::max(1, std::min(N / 2, (int)(cells / t.item_cells + 0.5)));
@@ -1012,17 +1018,19 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
     plan->stage_floats[l] = N * (ns * (TJ + 2) + ns * TJ);
     max_stage = std::max(max_stage, plan->stage_floats[l]);
     threads = std::max(threads, ((TJ * tpr + 31) / 32) * 32);
-    for (int j0 = 0; j0 < N; j0 += TJ)
+    for (int k = 0, j0 = 0; k < tiles; ++k) {
+      const int j1 = j0 + base + (k < rem ? 1 : 0);
       for (int i0 = 0; i0 < N; i0 += IC)
-        plan->items.push_back({l, level, j0, i0, std::min(N, i0 + IC)});
+        plan->items.push_back({l, level, j0, j1, i0, std::min(N, i0 + IC)});
+      j0 = j1;
+    }
   }
   // REAL before COMPLEX, largest first within a level: each free CTA takes
   // the next item (longest-processing-time order)
   std::stable_sort(plan->items.begin(), plan->items.end(),
                    [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
                      if (a.level != b.level) return a.level < b.level;
-                     return item_cost(a, plan->TJ[a.lattice], L[a.lattice].N) >
-                            item_cost(b, plan->TJ[b.lattice], L[b.lattice].N);
+                     return item_cost(a, L[a.lattice].N) > item_cost(b, L[b.lattice].N);
                    });
   plan->real_items = 0;
   for (const lfm::BatchItem& it : plan->items) plan->real_items += it.level == LFM_REAL;
@@ -1087,7 +1095,7 @@ int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_
       items_out[6 * k + 0] = it.level;
       items_out[6 * k + 1] = it.lattice;
       items_out[6 * k + 2] = it.j0;
-      items_out[6 * k + 3] = it.j0 + plan.TJ[it.lattice];
+      items_out[6 * k + 3] = it.j1;
       items_out[6 * k + 4] = it.i0;
       items_out[6 * k + 5] = it.i1;
     }

@@ -26,7 +26,7 @@ struct BatchLattice {
 struct BatchItem {
   int lattice;
   int level;  // LFM_REAL or LFM_COMPLEX, copied from the lattice
-  int j0, i0, i1;
+  int j0, j1, i0, i1;  // rows [j0, j1), planes [i0, i1)
 };
 
 struct BatchParams {

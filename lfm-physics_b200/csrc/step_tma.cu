@@ -1073,9 +1073,10 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
 // this step's parity, constants, mask table, tile shape) are built in shared
 // memory from the lattice descriptor.  The last CTA to retire rewinds the
 // counters for the next launch on the stream.
+// rows: the item's tile rows (the lattice's TJ or one fewer)
 template <int LEVEL>
 __device__ __forceinline__ void batch_params(TmaParams& P, const BatchLattice& L,
-                                             const BatchParams& B) {
+                                             const BatchParams& B, int rows) {
   const int cur = B.parity, nxt = 1 - B.parity;
   StepArgs a{};
   a.level = LEVEL;
@@ -1110,11 +1111,12 @@ __device__ __forceinline__ void batch_params(TmaParams& P, const BatchLattice& L
   P.pf_mask = -1;
   P.pf_sa = -1;
   P.N = L.N;
-  P.TJ = L.TJ;
+  P.TJ = rows;
   P.IC = L.IC;
   P.S = B.stages;
-  P.JT = L.N / L.TJ;
-  P.stage_floats = L.stage_floats;
+  P.JT = (L.N + L.TJ - 1) / L.TJ;
+  // a ragged tile's stages are smaller than the lattice's full ones (ns = np)
+  P.stage_floats = rows == L.TJ ? L.stage_floats : L.N * (2 * P.ns * rows + 2 * P.ns);
   P.tab_off = B.tab_off;  // after the largest ring of the batch, or -1
 }
 
@@ -1131,7 +1133,10 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
     const int w = s_item;
     if (w >= nitems) break;
     const BatchItem it = items[w];
-    if (threadIdx.x == 0) batch_params<LEVEL>(P, B.lattices[it.lattice], B);
+    if (threadIdx.x == 0) {
+      const BatchLattice& L = B.lattices[it.lattice];
+      batch_params<LEVEL>(P, L, B, it.j1 - it.j0);
+    }
     __syncthreads();  // P is visible to every thread
     q_march<LEVEL, V, false, true, GeomRTT<TABM>>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
     __syncthreads();  // every wait of the march is over
