@@ -151,15 +151,65 @@ class Evolver:
     sa_B = property(lambda s: s._buf("sa_B"))
 
     # ------------------------------------------------------------------
+    # live device views for per-step hooks (simulation.py:212-256)
+    # ------------------------------------------------------------------
+    def _view(self, t):
+        N = self.N
+        return t.view(N, N, N) if self._n_psi == 1 or t.numel() == N**3 else t.view(3, N, N, N)
+
+    def native_psi_real(self):
+        """The current Psi_r buffer as an (N, N, N) device view ((3, N, N, N) at COLOR):
+        edits are seen by the next step.  The previous-step buffers are not exposed."""
+        if self._mode == "ab":
+            return self._view(self._ab["psi_r_A" if self._use_buffer_A else "psi_r_B"])
+        return self._view(self._pr[self._cur])
+
+    def native_psi_imag(self):
+        """The current Psi_i buffer as a device view, None at the REAL level."""
+        if not self._has_imag:
+            return None
+        if self._mode == "ab":
+            return self._view(self._ab["psi_i_A" if self._use_buffer_A else "psi_i_B"])
+        return self._view(self._pi[self._cur])
+
+    def native_chi(self):
+        """The current chi buffer as an (N, N, N) device view."""
+        if self._mode == "ab":
+            return self._view(self._ab["chi_A" if self._use_buffer_A else "chi_B"])
+        return self._view(self._chi[self._cur])
+
+    def native_chi_pair(self):
+        """Every chi buffer a step reads, as device views: writing the same values to
+        all of them leaves chi without velocity there (the reference's four A/B buffers;
+        the resident layout's current and previous slots)."""
+        if self._mode == "ab":
+            return tuple(self._view(self._ab[k]) for k in ("chi_A", "chi_B", "chi_prev_A",
+                                                           "chi_prev_B"))
+        return (self._view(self._chi[self._cur]), self._view(self._chi[1 - self._cur]))
+
+    # ------------------------------------------------------------------
     # time loop (evolver.py:137-180)
     # ------------------------------------------------------------------
     use_graphs = True
     """Replay captured CUDA graphs of two steps when evolve() has no per-step host work."""
+    hook_block = 32
+    """Steps per captured graph when evolve() runs device hooks (even: parity returns)."""
 
-    def evolve(self, steps: int, callback=None, freeze_chi: bool = False) -> None:
-        """Run `steps` leapfrog steps; callback(evolver, step) every report_interval."""
+    def evolve(self, steps: int, callback=None, freeze_chi: bool = False, hooks=None) -> None:
+        """Run `steps` leapfrog steps; callback(evolver, step) every report_interval.
+
+        hooks: device hooks (lfm_b200.hooks) applied after every step, in order, as the
+        reference's per-step callbacks are; with no callback and no freeze_chi, blocks
+        of hook_block steps run as captured CUDA graphs together with their hooks.
+        """
         report = self.config.report_interval
-        if (callback is None and not freeze_chi and self._mode == "resident"
+        hooks = list(hooks or ())
+        if hooks:
+            if (callback is None and not freeze_chi and self._mode == "resident"
+                    and self.use_graphs and all(getattr(h, "graphable", False) for h in hooks)):
+                self._evolve_hooked(int(steps), hooks)
+                return
+        elif (callback is None and not freeze_chi and self._mode == "resident"
                 and self.use_graphs and steps >= 4):
             self._evolve_graphed(int(steps))
             return
@@ -180,8 +230,60 @@ class Evolver:
                     self._chi[self._cur].copy_(frozen[0])
                     self._chi[1 - self._cur].copy_(frozen[1])
             self.step += 1
+            for h in hooks:
+                h.apply(self, self.step)
             if callback is not None and report > 0 and self.step % report == 0:
                 callback(self, self.step)
+
+    def _evolve_hooked(self, steps: int, hooks) -> None:
+        """Steps with device hooks: whole blocks replay one captured graph each."""
+        K = int(self.hook_block) + (int(self.hook_block) % 2)
+        self._dt2 = self.config.dt**2
+        done = 0
+
+        def eager_step():
+            self._step()
+            self.step += 1
+            for h in hooks:
+                h.apply(self, self.step)
+
+        if not self._damp:  # the first step after a host write does not damp prev
+            eager_step()
+            done = 1
+        while steps - done >= K:
+            g = self._hook_graph(hooks, K)
+            for h in hooks:
+                h.begin_block(self, self.step, K)
+            g.replay()
+            for h in hooks:
+                h.end_block(self, K)
+            self.step += K
+            done += K
+        while done < steps:
+            eager_step()
+            done += 1
+
+    def _hook_graph(self, hooks, K: int):
+        import torch
+
+        if not hasattr(self, "_hgraphs"):
+            self._hgraphs = {}
+        key = (self._param_key(), K, tuple(id(h) for h in hooks))
+        g = self._hgraphs.get(key)
+        if g is None:
+            for h in hooks:
+                h.prepare_block(self, K)
+            saved = (self._cur, self._damp, self._use_buffer_A)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                for k in range(K):
+                    self._step_resident()
+                    self._use_buffer_A = not self._use_buffer_A
+                    for h in hooks:
+                        h.apply_in_block(self, k)
+            self._cur, self._damp, self._use_buffer_A = saved
+            self._hgraphs[key] = (g, list(hooks))  # the graph holds the hooks' buffers
+        return self._hgraphs[key][0]
 
     def _param_key(self) -> tuple:
         c = self.config

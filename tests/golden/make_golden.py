@@ -252,14 +252,67 @@ def checkpoint_fixture() -> None:
     sim.save_checkpoint(OUT / "ref_checkpoint.npz")
 
 
+HOOK_STEPS = 40
+HOOK_N = 16
+
+
+def hook_initial(level: str):
+    """The seeded initial Psi of the hooks fixture (also rebuilt by the tests)."""
+    rng = np.random.default_rng(7 if level == "real" else 8)
+    pr = (0.2 * rng.standard_normal((HOOK_N,) * 3)).astype(np.float32)
+    pi = (0.2 * rng.standard_normal((HOOK_N,) * 3)).astype(np.float32) if level == "complex" else None
+    return pr, pi
+
+
+def hooks_fixture() -> None:
+    """The reference's experiment hooks (Barrier with a which-path detector slit,
+    ContinuousSource, DetectorScreen) driving its Evolver for HOOK_STEPS steps,
+    the callbacks in the order of lfm/experiment/source.py's example."""
+    from lfm.config import FieldLevel, SimulationConfig
+    from lfm.experiment.barrier import Barrier, Slit
+    from lfm.experiment.detector import DetectorScreen
+    from lfm.experiment.source import ContinuousSource
+    from lfm.simulation import Simulation
+
+    data = {}
+    for level, fl in (("real", FieldLevel.REAL), ("complex", FieldLevel.COMPLEX)):
+        cfg = SimulationConfig(grid_size=HOOK_N, field_level=fl, report_interval=1)
+        sim = Simulation(cfg, backend="cpu")
+        pr, pi = hook_initial(level)
+        sim.set_psi_real(pr)
+        if pi is not None:
+            sim.set_psi_imag(pi)
+        slits = [Slit(center=5, width=3),
+                 Slit(center=11, width=3, detector=True, detector_strength=0.5)]
+        barrier = Barrier(sim, axis=2, position=HOOK_N // 2, thickness=2, slits=slits)
+        source = ContinuousSource(sim, axis=2, position=3, omega=19.05, amplitude=2.0,
+                                  envelope_sigma=0.25, phase=0.7, boost=10.0)
+        screen = DetectorScreen(sim, axis=2, position=12)
+
+        def cb(ev, step, sim=sim, barrier=barrier, source=source, screen=screen):
+            source.step_callback(sim, step)
+            barrier.step_callback(sim, step)
+            screen.record()
+
+        sim._evolver.evolve(HOOK_STEPS, callback=cb)
+        data[f"{level}_psi_real"] = sim.psi_real
+        if pi is not None:
+            data[f"{level}_psi_imag"] = sim.psi_imag
+        data[f"{level}_chi"] = sim.chi
+        data[f"{level}_frames"] = screen.snapshots
+        data[f"{level}_pattern"] = screen.pattern
+        data[f"{level}_barrier_mask"] = barrier.mask
+        data[f"{level}_slit_masks"] = np.stack(barrier.slit_masks)
+        data[f"{level}_envelope"] = source._envelope
+    np.savez_compressed(OUT / "hooks.npz", **data)
+
+
 if __name__ == "__main__":
-    masks()
-    stencil()
-    single_steps()
-    parity_runs()
-    metrics_fixture()
-    config1()
-    equilibrium_fixture()
-    sweep_fixture()
-    checkpoint_fixture()
+    import sys
+
+    every = [masks, stencil, single_steps, parity_runs, metrics_fixture, config1,
+             equilibrium_fixture, sweep_fixture, checkpoint_fixture, hooks_fixture]
+    chosen = [f for f in every if f.__name__ in sys.argv[1:]] or every
+    for f in chosen:
+        f()
     print("fixtures written to", OUT)
