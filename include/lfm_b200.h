@@ -225,6 +225,20 @@ int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const
                       int n_local, int i_first, double dt2, double kappa, double lambda_self,
                       double chi0, double e0_sq, double epsilon_w, void* stream);
 
+/* The slab step restricted to the slab's planes [plane_lo, plane_hi), 1 <=
+ * plane_lo < plane_hi <= n_local + 1 (lfm_slab_step_f32 is the range
+ * [1, n_local + 1)).  It lets a caller step the two boundary planes first,
+ * start their exchange with the neighbouring slabs, and step the interior
+ * planes while the exchange is in flight: the interior reads no ghost plane
+ * and writes none, and the new boundary planes are final once their range has
+ * run.  Each plane's bits are those of the whole-lattice step. */
+int lfm_slab_step_planes_f32(int level, const float* psi_r, float* psi_r_prev_io,
+                             const float* psi_i, float* psi_i_prev_io, const float* chi,
+                             float* chi_prev_io, const float* mask_table, const lfm_mask_lut* lut,
+                             int damp_prev, int N, int n_local, int i_first, int plane_lo,
+                             int plane_hi, double dt2, double kappa, double lambda_self,
+                             double chi0, double e0_sq, double epsilon_w, void* stream);
+
 /* Out-of-place form of lfm_leapfrog_real_f32 / lfm_leapfrog_complex_f32
  * (level LFM_REAL or LFM_COMPLEX): the same step and the same bits, with the
  * new fields written to *_out instead of over the previous ones, which stay

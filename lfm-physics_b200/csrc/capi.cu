@@ -575,6 +575,18 @@ int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const
                       const float* mask_table, const lfm_mask_lut* lut, int damp_prev, int N,
                       int n_local, int i_first, double dt2, double kappa, double lambda_self,
                       double chi0, double e0_sq, double epsilon_w, void* stream) {
+  return lfm_slab_step_planes_f32(level, psi_r, psi_r_prev_io, psi_i, psi_i_prev_io, chi,
+                                  chi_prev_io, mask_table, lut, damp_prev, N, n_local, i_first,
+                                  1, n_local + 1, dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w,
+                                  stream);
+}
+
+int lfm_slab_step_planes_f32(int level, const float* psi_r, float* psi_r_prev_io,
+                             const float* psi_i, float* psi_i_prev_io, const float* chi,
+                             float* chi_prev_io, const float* mask_table, const lfm_mask_lut* lut,
+                             int damp_prev, int N, int n_local, int i_first, int plane_lo,
+                             int plane_hi, double dt2, double kappa, double lambda_self,
+                             double chi0, double e0_sq, double epsilon_w, void* stream) {
   if (level != LFM_REAL && level != LFM_COMPLEX)
     return fail(LFM_ERR_UNSUPPORTED, "slab step: level %d (REAL and COMPLEX only)", level);
   int rc = check_n(N);
@@ -582,6 +594,9 @@ int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const
   if (n_local < 1 || i_first < 0 || i_first + n_local > N)
     return fail(LFM_ERR_INVALID_ARG, "slab planes [%d, %d) outside [0, %d)", i_first,
                 i_first + n_local, N);
+  if (plane_lo < 1 || plane_hi > n_local + 1 || plane_lo >= plane_hi)
+    return fail(LFM_ERR_INVALID_ARG, "slab plane range [%d, %d) outside [1, %d]", plane_lo,
+                plane_hi, n_local + 1);
   const bool cx = level == LFM_COMPLEX;
   if (!psi_r || !psi_r_prev_io || !chi || !chi_prev_io || (cx && (!psi_i || !psi_i_prev_io)))
     return fail(LFM_ERR_INVALID_ARG, "null buffer");
@@ -610,8 +625,8 @@ int lfm_slab_step_f32(int level, const float* psi_r, float* psi_r_prev_io, const
   a.damp_prev = damp_prev ? 1 : 0;
   a.slab = 1;
   a.ni = n_local + 2;
-  a.i_lo = 1;
-  a.i_hi = n_local + 1;
+  a.i_lo = plane_lo;
+  a.i_hi = plane_hi;
   a.i_off = i_first - 1;
   return run_step(a, static_cast<cudaStream_t>(stream));
 }

@@ -81,6 +81,8 @@ _SIGNATURES = {
     "lfm_metrics_f64_noalloc": [c_int] + [_P] * 5 + [c_int] + [_D] * 5 + [_P, _P],
     "lfm_slab_step_f32": [c_int] + [_P] * 7 + [POINTER(MaskLut), c_int, c_int, c_int, c_int]
     + [_D] * 6 + [_P],
+    "lfm_slab_step_planes_f32": [c_int] + [_P] * 7 + [POINTER(MaskLut)] + [c_int] * 6
+    + [_D] * 6 + [_P],
     "lfm_poisson_chi_f32": [_P, c_int, _P, _P, c_int] + [_D] * 4 + [c_int, _P, _P],
     "lfm_advance_f32": [c_int] + [_P] * 10 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6
     + [_P],

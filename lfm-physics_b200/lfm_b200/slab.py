@@ -10,7 +10,11 @@ After every step the ghost planes of the new fields are refreshed from the
 neighbouring slabs: one plane per stencil field per side (psi_r, psi_i, chi),
 sent with ``torch.distributed`` point-to-point operations (NCCL over NVLink
 between GPUs; gloo on CPU for the tests).  There is no other communication
-while stepping.
+while stepping.  With ``overlap`` (the default across ranks) a step runs the
+two boundary planes first (lfm_slab_step_planes_f32), starts their exchange,
+and steps the interior planes while it is in flight: the interior reads no
+ghost plane and writes none, so the exchange and the interior arithmetic
+proceed side by side and the step waits only for whichever ends last.
 
 Field accessors take and return the whole lattice (every rank passes the same
 host array to the setters, as each would to the reference's Evolver); getters
@@ -47,10 +51,14 @@ class SlabEvolver:
     """The planes [i_first, i_first + n_local) of one lattice, with ghost planes.
 
     rank / world default to torch.distributed's when it is initialised, else
-    0 / 1 (then the ghosts are the slab's own wrapped planes).  stepper replaces
-    the CUDA step (tests of the decomposition on the CPU); exchange replaces the
-    ghost refresh.  Slabs held by one process are stepped with evolve_local.
+    0 / 1 (then the ghosts are the slab's own wrapped planes).  stepper(slab,
+    lo, hi) replaces the CUDA step of the local planes [lo, hi) (tests of the
+    decomposition on the CPU); exchange replaces the ghost refresh.  Slabs held
+    by one process are stepped with evolve_local.
     """
+
+    overlap = True
+    """Across ranks: boundary planes, then their exchange beside the interior planes."""
 
     def __init__(self, config, backend="auto", rank: int | None = None,
                  world: int | None = None, group=None, device=None, stepper=None,
@@ -115,23 +123,40 @@ class SlabEvolver:
         return out
 
     # ---------------------------------------------------------------- stepping
-    def _step_local(self) -> None:
+    def _step_planes(self, lo: int, hi: int) -> None:
+        """Step the local planes [lo, hi) (1 <= lo < hi <= n_local + 1)."""
         if self._stepper is not None:
-            self._stepper(self)
+            self._stepper(self, lo, hi)
             return
         from .backend import _stream_handle
 
         c, p = self.cur, 1 - self.cur
         cfg = self.config
         ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
-        _lib.call("lfm_slab_step_f32", int(self.level), self.pr[c].data_ptr(),
+        _lib.call("lfm_slab_step_planes_f32", int(self.level), self.pr[c].data_ptr(),
                   self.pr[p].data_ptr(), ptr(self.pi[c] if self.cx else None),
                   ptr(self.pi[p] if self.cx else None), self.chi[c].data_ptr(),
                   self.chi[p].data_ptr(), self._table.data_ptr(), ctypes.byref(self._desc),
-                  1 if self.damp else 0, self.N, self.n_local, self.i_first,
+                  1 if self.damp else 0, self.N, self.n_local, self.i_first, int(lo), int(hi),
                   float(cfg.dt) ** 2, float(cfg.kappa), float(cfg.lambda_self),
                   float(cfg.chi0), float(cfg.e0_sq), float(cfg.epsilon_w),
                   _stream_handle(self.device))
+
+    def _step_local(self) -> None:
+        self._step_planes(1, self.n_local + 1)
+
+    def _start_exchange(self, slot: int) -> list:
+        """Post the ghost refresh of the fields in `slot`; returns the requests."""
+        import torch.distributed as dist
+
+        n = self.n_local
+        ops = []
+        for f in self.stencil_fields(slot):
+            ops.append(dist.P2POp(dist.isend, f[1], self.prev_rank, self.group, TAG_DOWN))
+            ops.append(dist.P2POp(dist.isend, f[n], self.next_rank, self.group, TAG_UP))
+            ops.append(dist.P2POp(dist.irecv, f[n + 1], self.next_rank, self.group, TAG_DOWN))
+            ops.append(dist.P2POp(dist.irecv, f[0], self.prev_rank, self.group, TAG_UP))
+        return dist.batch_isend_irecv(ops)
 
     def exchange(self) -> None:
         """Refresh the ghost planes of the current fields from the neighbours."""
@@ -139,25 +164,31 @@ class SlabEvolver:
             self._exchange_fn(self)
             return
         n = self.n_local
-        fields = self.stencil_fields(self.cur)
         if self.world == 1:
-            for f in fields:
+            for f in self.stencil_fields(self.cur):
                 f[0].copy_(f[n])
                 f[n + 1].copy_(f[1])
             return
-        import torch.distributed as dist
-
-        ops = []
-        for f in fields:
-            ops.append(dist.P2POp(dist.isend, f[1], self.prev_rank, self.group, TAG_DOWN))
-            ops.append(dist.P2POp(dist.isend, f[n], self.next_rank, self.group, TAG_UP))
-            ops.append(dist.P2POp(dist.irecv, f[n + 1], self.next_rank, self.group, TAG_DOWN))
-            ops.append(dist.P2POp(dist.irecv, f[0], self.prev_rank, self.group, TAG_UP))
-        for req in dist.batch_isend_irecv(ops):
+        for req in self._start_exchange(self.cur):
             req.wait()
 
     def advance(self, exchange: bool = True) -> None:
-        """One step of this slab, then (unless told not to) the ghost refresh."""
+        """One step of this slab, then (unless told not to) the ghost refresh; across
+        ranks with ``overlap``, the refresh runs beside the interior planes."""
+        n = self.n_local
+        if (exchange and self.overlap and self.world > 1 and n >= 3
+                and self._exchange_fn is None):
+            p = 1 - self.cur
+            self._step_planes(1, 2)
+            self._step_planes(n, n + 1)
+            reqs = self._start_exchange(p)  # the new boundary planes, in slot p
+            self._step_planes(2, n)
+            for req in reqs:
+                req.wait()
+            self.cur = p
+            self.damp = True
+            self.step += 1
+            return
         self._step_local()
         self.cur = 1 - self.cur
         self.damp = True
@@ -237,23 +268,37 @@ class SlabEvolver:
         return self.gather("chi")
 
 
-def exchange_local(slabs: list) -> None:
+def exchange_local(slabs: list, new: bool = False) -> None:
     """Ghost refresh between slabs held by one process (the ring of ranks
-    0 .. world-1, all on one device or on devices of this process)."""
+    0 .. world-1, all on one device or on devices of this process), of the
+    current fields, or with ``new`` of the fields a step is writing."""
     world = len(slabs)
+    slot = (lambda t: 1 - t.cur) if new else (lambda t: t.cur)  # noqa: E731
     for r, s in enumerate(slabs):
         nxt, prv = slabs[(r + 1) % world], slabs[(r - 1) % world]
         n = s.n_local
-        for f, fn, fp in zip(s.stencil_fields(s.cur), nxt.stencil_fields(nxt.cur),
-                             prv.stencil_fields(prv.cur)):
+        for f, fn, fp in zip(s.stencil_fields(slot(s)), nxt.stencil_fields(slot(nxt)),
+                             prv.stencil_fields(slot(prv))):
             f[n + 1].copy_(fn[1])
             f[0].copy_(fp[prv.n_local])
 
 
-def evolve_local(slabs: list, steps: int) -> None:
+def evolve_local(slabs: list, steps: int, overlap: bool = False) -> None:
     """Step slabs held by one process together: every slab, then one ghost
-    refresh among them, per step."""
+    refresh among them, per step.  With ``overlap`` each step runs the order
+    of the overlapped advance (boundary planes, refresh, interior planes)."""
     for _ in range(int(steps)):
+        if overlap and all(s.n_local >= 3 for s in slabs):
+            for s in slabs:
+                s._step_planes(1, 2)
+                s._step_planes(s.n_local, s.n_local + 1)
+            exchange_local(slabs, new=True)
+            for s in slabs:
+                s._step_planes(2, s.n_local)
+                s.cur = 1 - s.cur
+                s.damp = True
+                s.step += 1
+            continue
         for s in slabs:
             s.advance(exchange=False)
         exchange_local(slabs)

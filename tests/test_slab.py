@@ -34,12 +34,11 @@ def test_split_planes_covers_the_lattice(N, world):
 # A stand-in step that only needs the i-neighbours: new[p] = 1*cur[p-1] + 2*cur[p]
 # + 4*cur[p+1] + prev[p] on the slab's own planes (exact in float32 for small
 # integers), and the same stencil on the whole periodic lattice.
-def toy_step(slab):
+def toy_step(slab, lo, hi):
     c, p = slab.cur, 1 - slab.cur
-    n = slab.n_local
     for cur_f, prev_f in zip(slab.stencil_fields(c), slab.stencil_fields(p)):
-        new = cur_f[0:n] + 2 * cur_f[1:n + 1] + 4 * cur_f[2:n + 2] + prev_f[1:n + 1]
-        prev_f[1:n + 1].copy_(new)
+        new = cur_f[lo - 1:hi - 1] + 2 * cur_f[lo:hi] + 4 * cur_f[lo + 1:hi + 1] + prev_f[lo:hi]
+        prev_f[lo:hi].copy_(new)
 
 
 def toy_whole(cur, prev):
@@ -52,7 +51,7 @@ def _cfg(N, cx):
     return (gravity_em if cx else gravity_only)(N)
 
 
-def _gloo_worker(rank, world, port, N, cx, q):
+def _gloo_worker(rank, world, port, N, cx, overlap, q):
     import torch.distributed as dist
 
     from lfm_b200.slab import SlabEvolver
@@ -63,6 +62,7 @@ def _gloo_worker(rank, world, port, N, cx, q):
         rng = np.random.default_rng(3)
         a = rng.integers(-3, 4, size=(N, N, N)).astype(np.float32)
         s = SlabEvolver(_cfg(N, cx), stepper=toy_step, device="cpu")
+        s.overlap = overlap
         s.set_psi_real(a)
         s.set_chi(2 * a)
         if cx:
@@ -73,8 +73,11 @@ def _gloo_worker(rank, world, port, N, cx, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world, N, cx", [(2, 8, False), (3, 10, True)])
-def test_ghost_exchange_over_gloo_matches_the_whole_lattice(world, N, cx):
+@pytest.mark.parametrize("world, N, cx, overlap", [(2, 8, False, False), (3, 10, True, True),
+                                                   (2, 8, True, True), (3, 8, False, True)])
+def test_ghost_exchange_over_gloo_matches_the_whole_lattice(world, N, cx, overlap):
+    """With overlap the boundary planes step first and their exchange runs while
+    the interior planes step (N=8 over 3 ranks: one slab of 2 planes, too thin to overlap)."""
     import torch.multiprocessing as mp
 
     rng = np.random.default_rng(3)
@@ -90,7 +93,7 @@ def test_ghost_exchange_over_gloo_matches_the_whole_lattice(world, N, cx):
         port = sk.getsockname()[1]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_gloo_worker, args=(r, world, port, N, cx, q))
+    procs = [ctx.Process(target=_gloo_worker, args=(r, world, port, N, cx, overlap, q))
              for r in range(world)]
     for p in procs:
         p.start()
@@ -140,9 +143,11 @@ def _load(tgt, E, pi, chi):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("N, world", [(24, 1), (24, 3), (20, 2), (128, 4), (128, 3)])
+@pytest.mark.parametrize("N, world, overlap", [(24, 1, False), (24, 3, False), (20, 2, False),
+                                               (128, 4, False), (128, 3, False), (24, 3, True),
+                                               (128, 4, True), (20, 2, True)])
 @pytest.mark.parametrize("level", ["real", "complex"])
-def test_slabs_match_the_whole_lattice(be, N, world, level):
+def test_slabs_match_the_whole_lattice(be, N, world, overlap, level):
     from lfm_b200 import Evolver
     from lfm_b200.slab import SlabEvolver, evolve_local, gather_local
 
@@ -156,7 +161,7 @@ def test_slabs_match_the_whole_lattice(be, N, world, level):
         _load(s, E, pi, chi)
     steps = 7
     ev.evolve(steps)
-    evolve_local(slabs, steps)
+    evolve_local(slabs, steps, overlap=overlap)
     assert bits_equal(gather_local(slabs, "psi_r"), ev.get_psi_real())
     assert bits_equal(gather_local(slabs, "chi"), ev.get_chi())
     if cx:
