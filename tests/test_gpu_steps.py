@@ -232,12 +232,13 @@ def _seed(ev, level, E):
             ev.set_psi_imag(0.25 * E)
 
 
-@pytest.mark.parametrize("N", [20, 24, 48, 128, 256])
+@pytest.mark.parametrize("N", [20, 24, 48, 128, 256, 512])
 @pytest.mark.parametrize("level", ["real", "complex"])
 def test_resident_steps_bit_exact_at_every_kernel_shape(be, N, level):
     """Resident steps against the float32 oracle at sizes that reach each kernel
     variant: run-time tiles (24, 48), the direct fallback (20 COMPLEX), and the
-    compile-time tiles with packed two-cell arithmetic (128, 256)."""
+    compile-time tiles with packed two-cell arithmetic (128, 256, and 512, the
+    throughput workload's size)."""
     from lfm_b200 import Evolver
     from lfm_b200.config import gravity_em, gravity_only
 
