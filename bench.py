@@ -83,6 +83,15 @@ def measured_peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def workload_config(N: int, level: str) -> dict:
+    """The workload keys both arms report (the reference arm's line names the same
+    workload as this implementation's)."""
+    return {"workload": f"{level.upper()} {N}^3 leapfrog step (GOV-01 + GOV-02, 19-point, "
+                        "sponge), 64 packets, chi0 = 19 +- 1e-3",
+            "N": N, "level": level.upper(), "buffers": "resident",
+            "bytes_per_cell": 36 if level == "complex" else BYTES_PER_CELL["real"]}
+
+
 def profiled_traffic(N: int, level: str = "real"):
     """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "traffic.json"
@@ -237,8 +246,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"REAL {N}^3 leapfrog step, 64 packets", "N": N,
-                   "level": "REAL", "sample_planes_per_step": planes},
+        "config": dict(workload_config(N, "real"), sample_planes_per_step=planes),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
                          "sample": f"{planes} planes of the {N}^3 lattice per step"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -574,14 +582,11 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": f"{args.level.upper()} {N}^3 leapfrog step (GOV-01 + GOV-02, "
-                               "19-point, sponge), 64 packets, chi0 = 19 +- 1e-3",
-                   "N": N, "level": args.level.upper(), "buffers": "resident",
-                   "bytes_per_cell": bpc,
+        "config": dict(workload_config(N, args.level), **{
                    "l2": f"inputs {4 * bpc // 6 * cells / 1e9:.2f} GB"
                          + (" > L2, no flush" if 4 * bpc // 6 * cells > 126e6 else
                             " (within L2: profiling size only)"),
-                   "parallelism": f"independent lattices x{world}", "tile": cfg_used},
+                   "parallelism": f"independent lattices x{world}", "tile": cfg_used}),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": profiled_traffic(N, args.level),
