@@ -1,0 +1,140 @@
+"""Accuracy of the throughput workload against a float64 run of the reference
+step, and its energy drift.
+
+The workload is the REAL lattice with 64 packets (lfm_b200.workloads.real_solitons:
+chi = 19 +- 1e-3, amplitudes U[2, 6], sigma U[2, 4]).  The plain float32 Evolver
+and the compensated CompensatedEvolver run from the same state as a float64 run
+of the reference step (oracle/torch_ref.py: the reference's NumPy step,
+transcribed to torch, in float64 on the GPU).
+
+* Error: max-relative, max|x - x64| / max|x64|, for E and chi.
+* Energy: the reference's energy_total (lfm/analysis/energy.py:26-135, summed as
+  lfm/analysis/metrics.py:71-75 sums it).  The float32 paths take it from the
+  library's on-device float64 reduction.  The float64 run takes it from a float64
+  torch restatement of energy.py (energy64 below), which the test checks against
+  the device reduction on the same inputs.
+* Drift: the reference's energy_conservation_drift, |E_T - E_0| / |E_0| x 100.
+  The sponge absorbs the packets' outgoing waves, so the drift is mostly physics;
+  what float32 adds is the difference to the float64 run's drift.
+
+Run as a script for the full throughput configuration (512^3, 2000 steps):
+
+    python tests/test_gpu_accuracy.py 512 2000
+"""
+
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+for _p in (ROOT, ROOT / "lfm-physics_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+
+def _grad(f, axis: int):
+    """np.gradient along one axis: central differences inside, one-sided at the ends."""
+    import torch
+
+    g = torch.empty_like(f)
+    n = f.shape[axis]
+    mid = f.narrow(axis, 2, n - 2) - f.narrow(axis, 0, n - 2)
+    g.narrow(axis, 1, n - 2).copy_(mid / 2.0)
+    g.narrow(axis, 0, 1).copy_(f.narrow(axis, 1, 1) - f.narrow(axis, 0, 1))
+    g.narrow(axis, n - 1, 1).copy_(f.narrow(axis, n - 1, 1) - f.narrow(axis, n - 2, 1))
+    return g
+
+
+def energy64(pr, prp, chi, dt: float, c: float = 1.0) -> float:
+    """energy_total of energy.py in float64 for a REAL field (N, N, N) on the device."""
+    pr, prp, chi = (t.double() for t in (pr, prp, chi))
+    kinetic = 0.5 * ((pr - prp) / dt) ** 2
+    grad = sum(_grad(pr, ax) ** 2 for ax in range(3))
+    gradient = 0.5 * c * c * grad
+    potential = 0.5 * chi**2 * pr**2
+    return float(kinetic.sum() + gradient.sum() + potential.sum())
+
+
+def max_rel(a, ref) -> float:
+    return float((a.double() - ref).abs().max() / ref.abs().max().clamp_min(1e-300))
+
+
+def accuracy_report(N: int, steps: int, device: str = "cuda:0") -> dict:
+    import torch
+
+    from lfm_b200 import B200Backend, Evolver
+    from lfm_b200.compensated import CompensatedEvolver
+    from lfm_b200.config import gravity_only
+    from lfm_b200.mask import boundary_mask
+    from lfm_b200.workloads import real_solitons
+    from oracle import torch_ref as TR
+
+    cfg = gravity_only(N)
+    E, chi = real_solitons(N)
+    out = {"N": N, "steps": steps, "workload": "REAL, 64 packets, chi = 19 +- 1e-3"}
+
+    # float64 run of the reference step
+    dev = torch.device(device)
+    mask = torch.from_numpy(boundary_mask(N, cfg.boundary_fraction)).to(dev).double()
+    mask = mask.view(N, N, N)
+    e64 = torch.from_numpy(E).to(dev).double()
+    c64 = torch.from_numpy(chi).to(dev).double()
+    s = {"pr": e64, "prp": e64.clone(), "chi": c64, "chip": c64.clone()}
+    E0 = energy64(s["pr"], s["prp"], s["chi"], cfg.dt)
+    s = TR.run(cfg, s, steps, mask)
+    E1 = energy64(s["pr"], s["prp"], s["chi"], cfg.dt)
+    out["fp64"] = {"energy_0": E0, "energy_T": E1, "drift_percent": abs(E1 - E0) / abs(E0) * 100}
+
+    be = B200Backend(device)
+    for name, cls in (("plain_f32", Evolver), ("compensated_f32", CompensatedEvolver)):
+        ev = cls(cfg, backend=be)
+        ev.set_psi_real(E)
+        ev.set_chi(chi)
+        m0 = ev.metrics()["energy_total"]
+        ev.evolve(steps)
+        m1 = ev.metrics()["energy_total"]
+        st = ev.device_state()
+        pr = st["psi_r"].view(N, N, N)
+        ch = st["chi"].view(N, N, N)
+        out[name] = {
+            "max_rel_error_E": max_rel(pr, s["pr"]),
+            "max_rel_error_chi": max_rel(ch, s["chi"]),
+            "energy_0": m0, "energy_T": m1,
+            "drift_percent": abs(m1 - m0) / abs(m0) * 100,
+            # the device reduction against energy64 on the same float32 state
+            "energy_T_energy64": energy64(pr, st["psi_r_prev"].view(N, N, N), ch, cfg.dt),
+        }
+        out[name]["drift_minus_fp64_drift"] = (out[name]["drift_percent"]
+                                               - out["fp64"]["drift_percent"])
+        del ev, st, pr, ch
+        torch.cuda.empty_cache()
+    return out
+
+
+@pytest.mark.gpu
+def test_accuracy_and_energy_drift_of_the_throughput_workload(cuda_device):
+    """A reduced throughput workload (64^3, 200 steps): both float32 paths stay close
+    to float64, their energy drift matches the float64 run's, and the device energy
+    reduction agrees with the float64 restatement of energy.py."""
+    r = accuracy_report(64, 200, cuda_device)
+    print(json.dumps(r, indent=1))
+    for name in ("plain_f32", "compensated_f32"):
+        p = r[name]
+        assert p["energy_T"] == pytest.approx(p["energy_T_energy64"], rel=1e-9), name
+        # measured: E 2.6e-4 (compensated), chi 1.1e-4 (plain) / 5.2e-5 (compensated),
+        # drift differences 4e-5 percentage points or less
+        assert np.isfinite(p["max_rel_error_E"]) and p["max_rel_error_E"] < 2e-3, name
+        assert p["max_rel_error_chi"] < 5e-4, name
+        assert abs(p["drift_minus_fp64_drift"]) < 1e-3, name  # percentage points
+    assert r["compensated_f32"]["max_rel_error_chi"] <= r["plain_f32"]["max_rel_error_chi"]
+
+
+if __name__ == "__main__":
+    n = int(sys.argv[1]) if len(sys.argv) > 1 else 512
+    k = int(sys.argv[2]) if len(sys.argv) > 2 else 2000
+    print(json.dumps(accuracy_report(n, k), indent=1))
