@@ -17,9 +17,14 @@ transcribed to torch, in float64 on the GPU).
   The sponge absorbs the packets' outgoing waves, so the drift is mostly physics;
   what float32 adds is the difference to the float64 run's drift.
 
-Run as a script for the full throughput configuration (512^3, 2000 steps):
+The COLOR workload (full_physics, two colour-charged packets 40 cells apart,
+chi = 19 +- 1e-3, S_a solved every step) is reported per field: Re and Im of
+each colour, chi and S_a, against the same float64 transcription.
 
-    python tests/test_gpu_accuracy.py 512 2000
+Run as a script for the full configurations:
+
+    python tests/test_gpu_accuracy.py 512 2000          # REAL throughput workload
+    python tests/test_gpu_accuracy.py color 256 500     # COLOR workload
 """
 
 from __future__ import annotations
@@ -116,6 +121,53 @@ def accuracy_report(N: int, steps: int, device: str = "cuda:0") -> dict:
     return out
 
 
+def color_report(N: int, steps: int, device: str = "cuda:0") -> dict:
+    """Max-relative error per field of the COLOR path against float64."""
+    import torch
+
+    from lfm_b200 import B200Backend, Evolver
+    from lfm_b200.config import full_physics
+    from lfm_b200.mask import boundary_mask
+    from lfm_b200.workloads import color_packets
+    from oracle import torch_ref as TR
+
+    cfg = full_physics(N)
+    pr, pi, chi = color_packets(N)
+    dev = torch.device(device)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev).double()  # noqa: E731
+    mask = t(boundary_mask(N, cfg.boundary_fraction)).view(N, N, N)
+    s = {"pr": t(pr), "prp": t(pr), "pi": t(pi), "pip": t(pi), "chi": t(chi), "chip": t(chi)}
+    s = TR.run(cfg, s, steps, mask)
+    ev = Evolver(cfg, backend=B200Backend(device))
+    ev.set_psi_real(pr)
+    ev.set_psi_imag(pi)
+    ev.set_chi(chi)
+    ev.evolve(steps)
+    got = {"psi_real": torch.from_numpy(ev.get_psi_real()).to(dev),
+           "psi_imag": torch.from_numpy(ev.get_psi_imag()).to(dev),
+           "chi": torch.from_numpy(ev.get_chi()).to(dev),
+           "sa": torch.from_numpy(ev.get_sa_fields()).to(dev)}
+    out = {"N": N, "steps": steps,
+           "workload": "COLOR full_physics, two colour-charged packets, S_a every step"}
+    for a in range(3):
+        out[f"max_rel_error_psi_real_{a}"] = max_rel(got["psi_real"][a], s["pr"][a])
+        out[f"max_rel_error_psi_imag_{a}"] = max_rel(got["psi_imag"][a], s["pi"][a])
+        out[f"max_rel_error_sa_{a}"] = max_rel(got["sa"][a], s["sa"][a])
+    out["max_rel_error_chi"] = max_rel(got["chi"], s["chi"])
+    return out
+
+
+@pytest.mark.gpu
+def test_color_fields_against_float64(cuda_device):
+    """A reduced COLOR workload (32^3, 100 steps): every field within the stated
+    bound of float64 (cuFFT's float32 S_a included)."""
+    r = color_report(32, 100, cuda_device)
+    print(json.dumps(r, indent=1))
+    errs = {k: v for k, v in r.items() if k.startswith("max_rel")}
+    assert all(np.isfinite(v) for v in errs.values()), errs
+    assert max(errs.values()) < 1e-4, errs
+
+
 @pytest.mark.gpu
 def test_accuracy_and_energy_drift_of_the_throughput_workload(cuda_device):
     """A reduced throughput workload (64^3, 200 steps): both float32 paths stay close
@@ -135,6 +187,12 @@ def test_accuracy_and_energy_drift_of_the_throughput_workload(cuda_device):
 
 
 if __name__ == "__main__":
-    n = int(sys.argv[1]) if len(sys.argv) > 1 else 512
-    k = int(sys.argv[2]) if len(sys.argv) > 2 else 2000
-    print(json.dumps(accuracy_report(n, k), indent=1))
+    args = sys.argv[1:]
+    if args and args[0] == "color":
+        n = int(args[1]) if len(args) > 1 else 256
+        k = int(args[2]) if len(args) > 2 else 500
+        print(json.dumps(color_report(n, k), indent=1))
+    else:
+        n = int(args[0]) if args else 512
+        k = int(args[1]) if len(args) > 1 else 2000
+        print(json.dumps(accuracy_report(n, k), indent=1))
