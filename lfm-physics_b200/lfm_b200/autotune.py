@@ -44,7 +44,7 @@ def _store(key: str, value) -> None:
     data[key] = value
     try:
         p.parent.mkdir(parents=True, exist_ok=True)
-        tmp = p.with_suffix(".tmp")
+        tmp = p.with_suffix(f".{os.getpid()}.tmp")  # ranks on one host may store at once
         tmp.write_text(json.dumps(data, indent=1, sort_keys=True))
         tmp.replace(p)
     except OSError:
