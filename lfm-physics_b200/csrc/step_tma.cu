@@ -1323,19 +1323,20 @@ std::mutex KernelSlot<LEVEL, V, QUEUE, COMP>::mu;
 template <int LEVEL, int V, bool QUEUE, bool COMP>
 int KernelSlot<LEVEL, V, QUEUE, COMP>::granted = 0;
 
-// Compile-time tiles for the headline sizes (resident layout).
-template <int LEVEL, int V, int N, int TJ, int S>
+// Compile-time tiles for the headline sizes (resident layout); COMP: the
+// compensated (Delta-form) step on the same tile.
+template <int LEVEL, int V, int N, int TJ, int S, bool COMP = false>
 struct FixedSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
-    return tma_queue_kernel<LEVEL, V, false, GeomCT<N, TJ, QFields<LEVEL>::ns, S>>;
+    return tma_queue_kernel<LEVEL, V, COMP, GeomCT<N, TJ, QFields<LEVEL>::ns, S>>;
   }
 };
-template <int LEVEL, int V, int N, int TJ, int S>
-std::mutex FixedSlot<LEVEL, V, N, TJ, S>::mu;
-template <int LEVEL, int V, int N, int TJ, int S>
-int FixedSlot<LEVEL, V, N, TJ, S>::granted = 0;
+template <int LEVEL, int V, int N, int TJ, int S, bool COMP>
+std::mutex FixedSlot<LEVEL, V, N, TJ, S, COMP>::mu;
+template <int LEVEL, int V, int N, int TJ, int S, bool COMP>
+int FixedSlot<LEVEL, V, N, TJ, S, COMP>::granted = 0;
 
 struct FixedTile {
   int level, V, N, TJ, S;
@@ -1358,11 +1359,14 @@ const FixedTile* fixed_tile(int level, int V, int N) {
   return nullptr;
 }
 
-template <int LEVEL, int V, int N, int TJ>
+template <int LEVEL, int V, int N, int TJ, bool COMP = false>
 cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ)>;
+  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ), COMP>;
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
+
+// The compensated step has a compile-time tile at the throughput size only.
+constexpr bool comp_fixed(int level, int N) { return level == LFM_REAL && N == 512; }
 
 // Shared memory of the sponge table of the compile-time tiles: count entries
 // between a 0 and a 1, after 3 floats of padding that put the first entry on a
@@ -1372,14 +1376,21 @@ int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
 // Launches the compile-time variant when the chosen tile is one of
 // kFixedTiles (no streamed mask or S_a) and its ring plus the sponge table fit
 // in shared memory (ch.smem includes the table then); false if not.
-template <int LEVEL, int V>
+template <int LEVEL, int V, bool COMP = false>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
   if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
+  if (COMP && !comp_fixed(LEVEL, P.N)) return false;
   const FixedTile* t = fixed_tile(LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
   if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
     return false;
-  if constexpr (LEVEL == LFM_REAL && V == 4) {
+  if constexpr (COMP) {
+    if constexpr (LEVEL == LFM_REAL && V == 4) {
+      *err = launch_fixed<LEVEL, V, 512, 4, true>(P, ch, stream);
+      return true;
+    }
+    return false;
+  } else if constexpr (LEVEL == LFM_REAL && V == 4) {
     if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 4>(P, ch, stream); return true; }
     if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 8>(P, ch, stream); return true; }
     if (P.N == 128) { *err = launch_fixed<LEVEL, V, 128, 8>(P, ch, stream); return true; }
@@ -1410,8 +1421,8 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
   // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
-  const FixedTile* ft = (QUEUE && !COMP && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns &&
-                         !P.a.slab)
+  const FixedTile* ft = (QUEUE && (!COMP || comp_fixed(LEVEL, P.N)) && P.pf_mask < 0 &&
+                         P.pf_sa < 0 && P.np == P.ns && !P.a.slab)
                             ? fixed_tile(LEVEL, V, P.N) : nullptr;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {
@@ -1437,9 +1448,9 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   P.tab_off = tab_in_smem ? ch.S * P.stage_floats + 3 : -1;
   TileConfig used{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem, V};
   tune_record(LEVEL, P.N, used);
-  if constexpr (QUEUE && !COMP) {
+  if constexpr (QUEUE) {
     cudaError_t fe = cudaSuccess;
-    if (try_fixed<LEVEL, V>(P, ch, stream, &fe)) return fe;
+    if (try_fixed<LEVEL, V, COMP>(P, ch, stream, &fe)) return fe;
   }
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }

@@ -93,6 +93,36 @@ def test_compensated_fused_and_direct_paths_agree(be):
     assert max_rel(outs[0][1], outs[1][1]) < 1e-7
 
 
+def test_compensated_compile_time_tile_matches_run_time_tile(be):
+    """At 512^3 REAL the compensated step runs on the compile-time tile (4 rows, 3
+    stages); a forced run-time tile (2 rows) computes the same bits."""
+    import torch
+
+    from lfm_b200 import _lib
+    from lfm_b200.compensated import CompensatedEvolver
+    from lfm_b200.config import gravity_only
+    from lfm_b200.workloads import real_solitons
+
+    N = 512
+    E, chi = real_solitons(N)
+    outs = []
+    try:
+        for forced in (False, True):
+            _lib.tune_set(0, N, 2 if forced else 0, 3 if forced else 0)
+            ev = CompensatedEvolver(gravity_only(N), backend=be)
+            ev.set_psi_real(E)
+            ev.set_chi(chi)
+            ev.evolve(3)
+            assert _lib.tune_get(0, N)["tj"] == (2 if forced else 4)
+            outs.append([ev.get_psi_real(), ev.get_psi_real_prev(), ev.get_chi()])
+            del ev
+            torch.cuda.empty_cache()
+    finally:
+        _lib.tune_set(0, N, 0, 0)
+    for a, b in zip(*outs):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_compensated_accessors_round_trip(be):
     from lfm_b200.compensated import CompensatedEvolver
     from lfm_b200.config import gravity_em
