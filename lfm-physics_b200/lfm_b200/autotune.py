@@ -97,7 +97,7 @@ def _time_graph_ms(evolver, steps: int) -> float:
 # ------------------------------------------------------------------ batches
 BATCH_CANDIDATES = [
     dict(threads=t, stages=s, item_cells=c)
-    for t, s, c in itertools.product((128, 256, 512), (3, 4), (16384, 32768, 65536, 131072))
+    for t, s, c in itertools.product((128, 256, 512), (3, 4, 5), (16384, 32768, 65536, 131072))
 ]
 
 
