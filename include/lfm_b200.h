@@ -377,10 +377,11 @@ int lfm_metrics_f64_noalloc(int level, const float* psi_r, const float* psi_r_pr
 int lfm_set_step_path(int path);
 
 /* Tile configuration of the fused kernel for (level, N): cells per thread
- * along k (vec: 2 or 4, 0 = automatic), rows per tile, shared-memory stages
- * and planes per chunk (ic 0 = automatic).  tj <= 0 removes the entry and
- * restores the built-in choice.  lfm_tune_get reports the configuration the
- * last fused step of that (level, N) ran with. */
+ * along k (vec: 2 or 4 at REAL and COMPLEX, 1 or 2 at COLOR, 0 = automatic;
+ * the fused kernel refuses other widths, like any tile it cannot run), rows per tile,
+ * shared-memory stages and planes per chunk (ic 0 = automatic).  tj <= 0
+ * removes the entry and restores the built-in choice.  lfm_tune_get reports
+ * the configuration the last fused step of that (level, N) ran with. */
 int lfm_tune_set(int level, int N, int vec, int tj, int stages, int ic);
 int lfm_tune_get(int level, int N, int* vec, int* tj, int* stages, int* ic, int* threads,
                  int* smem);

@@ -1521,17 +1521,22 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   }
   if (a.level == LFM_REAL) {
     const int v = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 4;
-    if (N % v) return cudaErrorNotSupported;
+    if ((v != 2 && v != 4) || N % v) return cudaErrorNotSupported;
     return v == 2 ? plan_and_launch<LFM_REAL, 2, true>(P, forced, stream)
                   : plan_and_launch<LFM_REAL, 4, true>(P, forced, stream);
   }
   if (a.level == LFM_COMPLEX) {
     const int v = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 2;
-    if (N % v) return cudaErrorNotSupported;
+    if ((v != 2 && v != 4) || N % v) return cudaErrorNotSupported;
     return v == 4 ? plan_and_launch<LFM_COMPLEX, 4, true>(P, forced, stream)
                   : plan_and_launch<LFM_COMPLEX, 2, true>(P, forced, stream);
   }
-  return plan_and_launch<LFM_COLOR, 2, false>(P, forced, stream);
+  // COLOR: two cells per lane, or one when a tuning asks for it (twice the
+  // warps on the same ring, each with half the independent arithmetic)
+  const int vc = (have_forced && forced_cfg.vec) ? forced_cfg.vec : 2;
+  if (vc != 1 && vc != 2) return cudaErrorNotSupported;
+  return vc == 1 ? plan_and_launch<LFM_COLOR, 1, false>(P, forced, stream)
+                 : plan_and_launch<LFM_COLOR, 2, false>(P, forced, stream);
 }
 
 

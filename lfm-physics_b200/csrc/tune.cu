@@ -37,7 +37,7 @@ int lfm_tune_set(int level, int N, int vec, int tj, int stages, int ic) {
     lfm::g_forced.erase({level, N});
     return LFM_OK;
   }
-  if (vec != 0 && vec != 2 && vec != 4) return LFM_ERR_INVALID_ARG;
+  if (vec != 0 && vec != 1 && vec != 2 && vec != 4) return LFM_ERR_INVALID_ARG;
   lfm::g_forced[{level, N}] = lfm::TileConfig{tj, stages, ic, 0, 0, vec};
   return LFM_OK;
 }

@@ -147,7 +147,7 @@ def lattice_candidates(level: int):
     """Vector width x rows per tile x stages x plane chunk (0 = the planner's
     wave-balanced chunk).  Small lattices are latency-bound: deep rings and
     short chunks (many CTAs, few planes each) pay there."""
-    vecs = (4, 2) if level == 0 else (2,)
+    vecs = {0: (4, 2), 1: (2,), 2: (2, 1)}[level]
     return [dict(vec=v, tj=tj, stages=s, ic=ic)
             for v, tj, s, ic in itertools.product(vecs, (1, 2, 4, 8), (3, 4, 6),
                                                   (0, 4, 8, 16, 32, 64))]

@@ -118,6 +118,48 @@ def test_protocol_step_color_bit_exact(be, path, N, couplings):
         assert bits_equal(be.to_numpy(d), r), f"output {k}"
 
 
+@pytest.mark.parametrize("N,tj", [(16, 4), (32, 2), (64, 2)])
+def test_color_one_cell_per_lane_bit_exact(be, N, tj):
+    """The COLOR kernel with one cell per lane (a tuning option), on the streamed
+    mask of the protocol step and on the resident layout's table, against the oracle."""
+    from lfm_b200 import Evolver, _lib
+
+    rng = np.random.default_rng(250 + N)
+    n = N**3
+    ins = rand_fields(rng, n, [(1, 0, 3)] * 4 + [(0.5, CHI0, 1)] * 2)
+    mask = O.boundary_mask(N, 0.3)
+    shapes = [3 * n] * 4 + [n, n]
+    ref = [np.empty(s, np.float32) for s in shapes]
+    O.OracleBackend().step_color(*ins, mask, *ref, N, DT2, KAPPA, LAMBDA_H, CHI0, 0.0, 0.1,
+                                 CC["kappa_c"], CC["epsilon_cc"], kappa_string=CC["kappa_string"])
+    _lib.set_step_path(_lib.PATH_FUSED)
+    try:
+        _lib.tune_set(2, N, tj, 4, 0, 1)
+        d_in = [be.from_numpy(a) for a in ins]
+        d_out = [be.from_numpy(np.zeros(s, np.float32)) for s in shapes]
+        be.step_color(*d_in, be.from_numpy(mask), *d_out, N, DT2, KAPPA, LAMBDA_H, CHI0, 0.0,
+                      0.1, CC["kappa_c"], CC["epsilon_cc"], kappa_string=CC["kappa_string"])
+        assert _lib.tune_get(2, N)["vec"] == 1
+        for k, (r, d) in enumerate(zip(ref, d_out)):
+            assert bits_equal(be.to_numpy(d), r), f"output {k}"
+
+        cfg = _parity_config("color", sa=False, N=N)
+        E = O.parity_seed_blob(N)
+        ev = Evolver(cfg, backend=be)
+        lat = O.OracleLattice(cfg)
+        _seed(ev, "color", E)
+        _seed(lat, "color", E)
+        ev.evolve(12)
+        lat.step(12)
+        assert _lib.tune_get(2, N)["vec"] == 1
+        assert bits_equal(ev.get_psi_real().ravel(), lat.pr)
+        assert bits_equal(ev.get_psi_imag().ravel(), lat.pi)
+        assert bits_equal(ev.get_chi().ravel(), lat.chi)
+    finally:
+        _lib.tune_set(2, N, 0, 0)
+        _lib.set_step_path(_lib.PATH_AUTO)
+
+
 @pytest.mark.parametrize("N", [12, 16, 32])
 def test_protocol_step_color_with_sa(be, N):
     """Psi outputs stay bit-exact; S_a and chi within the stated tolerances."""
@@ -206,15 +248,15 @@ def test_wrong_dtype_and_size_rejected(be):
 # ----------------------------------------------------------------------------
 # Evolver runs against the reference fixtures
 # ----------------------------------------------------------------------------
-def _parity_config(level: str, sa: bool = True):
+def _parity_config(level: str, sa: bool = True, N: int = 16):
     from lfm_b200.config import FieldLevel, SimulationConfig
 
     if level == "real":
-        return SimulationConfig(grid_size=16, boundary_fraction=0.15)
+        return SimulationConfig(grid_size=N, boundary_fraction=0.15)
     if level == "complex":
-        return SimulationConfig(grid_size=16, boundary_fraction=0.15,
+        return SimulationConfig(grid_size=N, boundary_fraction=0.15,
                                 field_level=FieldLevel.COMPLEX, lambda_self=LAMBDA_H)
-    return SimulationConfig(grid_size=16, boundary_fraction=0.15, field_level=FieldLevel.COLOR,
+    return SimulationConfig(grid_size=N, boundary_fraction=0.15, field_level=FieldLevel.COLOR,
                             lambda_self=LAMBDA_H, kappa_tube=KT if sa else 0.0, **CC)
 
 
