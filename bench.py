@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--batch-tuning", default="auto",
                     help="auto (the autotuner), default, or THREADS,STAGES,ITEM_CELLS")
     ap.add_argument("--adjoint-steps", type=int, default=500)
+    ap.add_argument("--no-color", action="store_true")
+    ap.add_argument("--color-N", type=int, default=256)
+    ap.add_argument("--color-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -350,6 +353,65 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
                          "trials": len(tune.get("trials", []))}}
 
 
+def run_color(args, be, dev, world, barrier, max_over_ranks, peak):
+    """COLOR step (full_physics, three complex colours, S_a solved every step) on two
+    colour-charged packets 40 cells apart with chi = 19 +- 1e-3, device-timed over
+    `color_steps` graph-replayed steps on every rank (its own lattice each).  The fused stencil kernel moves 84 B/cell
+    (Psi_a, chi and their previous values in, new values out) plus 12 B/cell of S_a;
+    the S_a solve adds |Psi_a|^2, three R2C/C2R cuFFT pairs and the k-space filter.
+    The same lattice without the tube coupling (kappa_tube = 0, no S_a) is timed
+    beside it to split the step."""
+    import torch
+
+    from lfm_b200 import Evolver, _lib
+    from lfm_b200.config import full_physics
+    from lfm_b200.workloads import color_packets
+
+    N, steps = args.color_N, args.color_steps
+    pr, pi, chi = color_packets(N)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(cfg):
+        ev = Evolver(cfg, backend=be)
+        ev.set_psi_real(pr)
+        ev.set_psi_imag(pi)
+        ev.set_chi(chi)
+        ev.evolve(max(args.warmup, 4))
+        ev.warm_graphs()
+        torch.cuda.synchronize(dev)
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ev.evolve(steps)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ms = max_over_ranks(a.elapsed_time(b)) / steps
+        del ev
+        torch.cuda.empty_cache()
+        return ms
+
+    ms = timed(full_physics(N))
+    tile = _lib.tune_get(2, N)
+    ms_no_sa = timed(full_physics(N, kappa_tube=0.0))
+    status = _lib.device_status(clear=True)
+    if status:
+        raise RuntimeError(f"device status word {status} after the COLOR steps")
+    cells = N**3
+    stencil = 84 * cells / (ms_no_sa / 1e3) / 1e9  # without the tube coupling: no S_a read
+    return {"workload": f"COLOR {N}^3 full_physics, two colour-charged packets 40 cells apart, "
+                        "S_a every step",
+            "value": world * cells / (ms / 1e3) / 1e9, "unit": METRIC, "ms_per_step": ms,
+            "steps": steps, "tile": tile,
+            "without_sa": {"ms_per_step": ms_no_sa,
+                           "value": world * cells / (ms_no_sa / 1e3) / 1e9,
+                           "roofline": {"bound": "hbm", "achieved": stencil, "peak": peak,
+                                        "unit": "GB/s", "frac": stencil / peak,
+                                        "bytes_per_cell": 84}},
+            "sa_ms_per_step": ms - ms_no_sa}
+
+
 def run_adjoint(args, be, dev, barrier, max_over_ranks):
     """Gradient of |chi_final - chi_target|^2 through `adjoint_steps` COMPLEX 96^3
     steps (gravity_em: lambda = 4/31, eps_w = 0.1) with respect to the
@@ -532,6 +594,10 @@ def run_b200(args):
                 "tile": _lib.tune_get(0, N)}
         del evc
 
+    color = None
+    if not args.no_color:
+        color = run_color(args, be, dev, world, barrier, max_over_ranks, peak)
+
     adjoint = None
     if not args.no_adjoint:
         adjoint = run_adjoint(args, be, dev, barrier, max_over_ranks)
@@ -602,6 +668,8 @@ def run_b200(args):
         line["batched"] = batched
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if color is not None:
+        line["color"] = color
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
     if world > 1:

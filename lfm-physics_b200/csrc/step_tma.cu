@@ -190,6 +190,24 @@ __device__ __forceinline__ void stg(float* p, const float (&x)[V]) {
   }
 }
 
+// Coherent vector load from global memory (the point fields of the
+// barrier kernel; in the resident layout a thread reads its own prev cells
+// and then overwrites them, so the read-only path is not used).
+template <int V>
+__device__ __forceinline__ Vec<V> ldgv(const float* p) {
+  Vec<V> r;
+  if constexpr (V == 4) {
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+  } else if constexpr (V == 2) {
+    const float2 t = *reinterpret_cast<const float2*>(p);
+    r.v[0] = t.x; r.v[1] = t.y;
+  } else {
+    r.v[0] = *p;
+  }
+  return r;
+}
+
 // Per-thread geometry inside the tile.
 struct Lane {
   int r;        // tile row (0..TJ-1)
@@ -278,14 +296,12 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
   const StepArgs& a = P.a;
   const int N = P.N, TJ = P.TJ;
   const int field_rows = (TJ + 2) * N;
-  const int point_base = P.ns * field_rows;
-  const int pt = point_base + L.r * N + L.k0;  // + g*TJ*N for point field g
   const int64_t gofs = ((int64_t)i * N + j) * N + L.k0;
 
   // sponge factor per cell
   float mask[V], absorb[V];
   if (P.pf_mask >= 0) {
-    const Vec<V> m = lds<V>(smem, s0 + pt + P.pf_mask * TJ * N);
+    const Vec<V> m = ldgv<V>(P.pf[P.pf_mask] + gofs);
 #pragma unroll
     for (int e = 0; e < V; ++e) mask[e] = m.v[e];
   } else {
@@ -296,13 +312,15 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
 #pragma unroll
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
 
+  // Point fields (previous values, mask, S_a) are read once per cell, from
+  // global memory; only the stencil fields go through the shared-memory ring.
   auto prev = [&](int g, float (&out)[V]) {
-    const Vec<V> p = lds<V>(smem, s0 + pt + g * TJ * N);
+    const Vec<V> p = ldgv<V>(P.pf[g] + gofs);
 #pragma unroll
     for (int e = 0; e < V; ++e) out[e] = a.damp_prev ? fmul(p.v[e], absorb[e]) : p.v[e];
   };
   auto plain = [&](int g, float (&out)[V]) {
-    const Vec<V> p = lds<V>(smem, s0 + pt + g * TJ * N);
+    const Vec<V> p = ldgv<V>(P.pf[g] + gofs);
 #pragma unroll
     for (int e = 0; e < V; ++e) out[e] = p.v[e];
   };
@@ -353,10 +371,21 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
   } else {
     const int64_t n3 = (int64_t)N * N * N;
     // stencil fields: R0 R1 R2 I0 I1 I2 chi ; point fields: Rp0..2 Ip0..2 chip [mask] [S0..2]
-    float lapX[V], cX[V], xp[V];
+    // the point loads first: their latency runs under the stencil arithmetic
+    float lapX[V], cX[V], xp[V], rpc[3][V], ipc[3][V], sac[3][V];
+    plain(6, xp);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      prev(c, rpc[c]);
+      prev(3 + c, ipc[c]);
+    }
+    const bool has_sa = P.pf_sa >= 0;
+    if (has_sa) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) plain(P.pf_sa + c, sac[c]);
+    }
     field_stencil<V, false>(smem, sm + 6 * field_rows, s0 + 6 * field_rows, sp + 6 * field_rows,
                             N, L, lapX, cX, nofaces);
-    plain(6, xp);
     ColorAcc A[V];
     {
       Vec<V> cr[3], ci[3];
@@ -374,20 +403,18 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      float lapR[V], cR[V], lapI[V], cI[V], rp[V], ip[V];
+      float lapR[V], cR[V], lapI[V], cI[V];
       Faces fR[V], fI[V];
       field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
                              N, L, lapR, cR, fR);
       field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
                              sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
-      prev(c, rp);
-      prev(3 + c, ip);
       float o_r[V], o_i[V], o_rp[V], o_ip[V];
 #pragma unroll
       for (int e = 0; e < V; ++e) {
         const ColorCompOut o =
-            color_component(A[e], c, lapR[e], cR[e], rp[e], fR[e], lapI[e], cI[e], ip[e], fI[e],
-                            a.c);
+            color_component(A[e], c, lapR[e], cR[e], rpc[c][e], fR[e], lapI[e], cI[e], ipc[c][e],
+                            fI[e], a.c);
         o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
       }
       stg<V>(a.pr_out + c * n3 + gofs, o_r);
@@ -396,12 +423,12 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
       if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
     }
     float sa[V][3];
-    const bool has_sa = P.pf_sa >= 0;
     if (has_sa) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         float t[V];
-        plain(P.pf_sa + c, t);
+#pragma unroll
+        for (int e = 0; e < V; ++e) t[e] = sac[c][e];
 #pragma unroll
         for (int e = 0; e < V; ++e) sa[e][c] = t[e];
         if (a.sa_clip_out) {
@@ -419,8 +446,11 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
   }
 }
 
-// Copies plane (i0 - 1 + u) into stage u % S.
-template <bool SLAB = true>
+// Copies plane (i0 - 1 + u) into stage u % S: the stencil fields' tile rows
+// and halo rows, and with PT the point fields' tile rows (the register-queue
+// kernels read them from the stage; the barrier kernel reads them from global
+// memory).
+template <bool SLAB = true, bool PT = true>
 __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                             int u, int i0, int i1, int j0) {
   const int N = P.N, TJ = P.TJ;
@@ -428,7 +458,7 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
   const int pw = (SLAB && P.a.slab) ? p : (p % N + N) % N;  // slabs read their ghost planes
   const int s = u % P.S;
   float* st = smem + (size_t)s * P.stage_floats;
-  const bool point = (p >= i0) && (p < i1);
+  const bool point = PT && (p >= i0) && (p < i1);
   const uint32_t row_bytes = 4u * (uint32_t)N;
   const uint32_t bytes =
       row_bytes * (uint32_t)(P.ns * (TJ + 2) + (point ? P.np * TJ : 0));
@@ -484,7 +514,8 @@ __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ T
   __syncthreads();
   int issued = 0;
   if (tid == 0) {
-    for (; issued < min(S, nplanes); ++issued) issue_plane(P, smem, bars, issued, i0, i1, j0);
+    for (; issued < min(S, nplanes); ++issued)
+      issue_plane<true, false>(P, smem, bars, issued, i0, i1, j0);
   }
 
   int waited = 0;
@@ -505,7 +536,7 @@ __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ T
     __syncthreads();
     if (abort_flag) break;
     if (tid == 0 && c + S < nplanes) {
-      issue_plane(P, smem, bars, c + S, i0, i1, j0);
+      issue_plane<true, false>(P, smem, bars, c + S, i0, i1, j0);
       issued = c + S + 1;
     }
   }
@@ -1431,19 +1462,20 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   }
   const int planes = P.a.slab ? P.a.i_hi - P.a.i_lo : P.N;
   bool tab_in_smem = want_tab;
-  Choice ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, tab_smem, 0,
-                     planes);
+  const int np_staged = QUEUE ? P.np : 0;  // the barrier kernel reads point fields from global
+  Choice ch = choose(LEVEL, P.N, V, P.ns, np_staged, QUEUE, max_threads, regs, forced, tab_smem,
+                     0, planes);
   if (!ch.TJ && want_tab) {  // the table does not fit beside any ring: through L1
     tab_in_smem = false;
-    ch = choose(LEVEL, P.N, V, P.ns, P.np, QUEUE, max_threads, regs, forced, 0, table_bytes,
-                planes);
+    ch = choose(LEVEL, P.N, V, P.ns, np_staged, QUEUE, max_threads, regs, forced, 0,
+                table_bytes, planes);
   }
   if (!ch.TJ) return cudaErrorNotSupported;
   P.TJ = ch.TJ;
   P.S = ch.S;
   P.IC = ch.IC;
   P.JT = P.N / ch.TJ;
-  P.stage_floats = stage_bytes(P.N, ch.TJ, P.ns, P.np) / 4;
+  P.stage_floats = stage_bytes(P.N, ch.TJ, P.ns, np_staged) / 4;
   // tab[1] lands on a 16-byte boundary: stage_floats is a multiple of N, N of 4
   P.tab_off = tab_in_smem ? ch.S * P.stage_floats + 3 : -1;
   TileConfig used{ch.TJ, ch.S, ch.IC, ch.threads, ch.smem, V};
