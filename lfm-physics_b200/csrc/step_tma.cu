@@ -6,11 +6,14 @@
 // copies (cp.async.bulk) completing on an mbarrier:
 //   * every stencil field (Psi components and chi): the TJ tile rows plus
 //     the two periodic halo rows j0-1 and j0+TJ -> TJ+2 rows of N floats;
-//   * every point field (previous-step fields, the protocol mask, S_a):
-//     the TJ tile rows.
-// into one stage of an S-deep shared-memory ring.  Computing plane i reads
-// the stages of planes i-1, i, i+1; after a CTA barrier the stage of i-1 is
-// refilled with plane i-1+S, so S-3 planes stream in while one is computed.
+//   * in the register-queue kernels (REAL, COMPLEX, the batch), every point
+//     field (previous-step fields, the protocol mask): the TJ tile rows
+// into one stage of an S-deep shared-memory ring.  The barrier kernel
+// (COLOR, below) stages only its seven stencil fields and reads the point
+// fields (previous-step fields, mask, S_a) once per cell from global memory.
+// There, computing plane i reads the stages of planes i-1, i, i+1; after a
+// CTA barrier the stage of i-1 is refilled with plane i-1+S, so S-3 planes
+// stream in while one is computed.
 // Periodic wrap in i and j is folded into the copy addresses; wrap in k is
 // resolved when reading shared memory.  Each thread updates V consecutive
 // cells of one row with vector loads/stores; its k-1 / k+V neighbours come
