@@ -457,7 +457,7 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
         barrier()
         fwd = max_over_ranks(ev[0].elapsed_time(ev[1]))
         bwd = max_over_ranks(ev[1].elapsed_time(ev[2]))
-        return fwd, bwd, float(loss), [float(q.grad.abs().max()) for q in p] + [
+        return fwd, bwd, float(loss.detach()), [float(q.grad.abs().max()) for q in p] + [
             float(dchi.grad.abs().max())]
 
     one(False)
