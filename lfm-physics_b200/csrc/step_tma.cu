@@ -293,9 +293,11 @@ __device__ __forceinline__ void field_stencil(const float* smem, int fm, int f0,
   }
 }
 
-template <int LEVEL, int V>
-__device__ __forceinline__ void compute_plane(const TmaParams& P, const float* smem, int sm,
-                                              int s0, int sp, int i, const Lane& L, int j) {
+// One output plane of the COLOR step: seven 19-point stencils from the
+// ring, the point fields from global memory, lfm_cells.cuh's colour update.
+template <int V>
+__device__ __forceinline__ void color_plane(const TmaParams& P, const float* smem, int sm, int s0,
+                                            int sp, int i, const Lane& L, int j) {
   const StepArgs& a = P.a;
   const int N = P.N, TJ = P.TJ;
   const int field_rows = (TJ + 2) * N;
@@ -329,124 +331,80 @@ __device__ __forceinline__ void compute_plane(const TmaParams& P, const float* s
   };
 
   Faces nofaces[V];
-  if constexpr (LEVEL == LFM_REAL) {
-    float lapE[V], cE[V], lapX[V], cX[V], ep[V], xp[V];
-    field_stencil<V, false>(smem, sm, s0, sp, N, L, lapE, cE, nofaces);
-    field_stencil<V, false>(smem, sm + field_rows, s0 + field_rows, sp + field_rows, N, L, lapX,
-                            cX, nofaces);
-    prev(0, ep);
-    plain(1, xp);
-    float o_psi[V], o_chi[V], o_pp[V], o_cp[V];
+  const int64_t n3 = (int64_t)N * N * N;
+  // stencil fields: R0 R1 R2 I0 I1 I2 chi ; point fields: Rp0..2 Ip0..2 chip [mask] [S0..2]
+  // the point loads first: their latency runs under the stencil arithmetic
+  float lapX[V], cX[V], xp[V], rpc[3][V], ipc[3][V], sac[3][V];
+  plain(6, xp);
 #pragma unroll
-    for (int e = 0; e < V; ++e) {
-      const RealOut o = real_cell(lapE[e], cE[e], ep[e], lapX[e], cX[e], xp[e], mask[e], a.c);
-      o_psi[e] = o.psi; o_chi[e] = o.chi; o_pp[e] = o.psi_prev; o_cp[e] = o.chi_prev;
-    }
-    stg<V>(a.pr_out + gofs, o_psi);
-    stg<V>(a.chi_out + gofs, o_chi);
-    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_pp);
-    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
-  } else if constexpr (LEVEL == LFM_COMPLEX) {
-    float lapR[V], cR[V], lapI[V], cI[V], lapX[V], cX[V], rp[V], ip[V], xp[V];
-    Faces fR[V], fI[V];
-    field_stencil<V, true>(smem, sm, s0, sp, N, L, lapR, cR, fR);
-    field_stencil<V, true>(smem, sm + field_rows, s0 + field_rows, sp + field_rows, N, L, lapI,
-                           cI, fI);
-    field_stencil<V, false>(smem, sm + 2 * field_rows, s0 + 2 * field_rows, sp + 2 * field_rows,
-                            N, L, lapX, cX, nofaces);
-    prev(0, rp);
-    prev(1, ip);
-    plain(2, xp);
-    float o_r[V], o_i[V], o_c[V], o_rp[V], o_ip[V], o_cp[V];
-#pragma unroll
-    for (int e = 0; e < V; ++e) {
-      const ComplexOut o = complex_cell(lapR[e], cR[e], rp[e], fR[e], lapI[e], cI[e], ip[e],
-                                        fI[e], lapX[e], cX[e], xp[e], mask[e], a.c);
-      o_r[e] = o.pr; o_i[e] = o.pi; o_c[e] = o.chi;
-      o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev; o_cp[e] = o.chi_prev;
-    }
-    stg<V>(a.pr_out + gofs, o_r);
-    stg<V>(a.pi_out + gofs, o_i);
-    stg<V>(a.chi_out + gofs, o_c);
-    if (a.pr_prev_out) stg<V>(a.pr_prev_out + gofs, o_rp);
-    if (a.pi_prev_out) stg<V>(a.pi_prev_out + gofs, o_ip);
-    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, o_cp);
-  } else {
-    const int64_t n3 = (int64_t)N * N * N;
-    // stencil fields: R0 R1 R2 I0 I1 I2 chi ; point fields: Rp0..2 Ip0..2 chip [mask] [S0..2]
-    // the point loads first: their latency runs under the stencil arithmetic
-    float lapX[V], cX[V], xp[V], rpc[3][V], ipc[3][V], sac[3][V];
-    plain(6, xp);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      prev(c, rpc[c]);
-      prev(3 + c, ipc[c]);
-    }
-    const bool has_sa = P.pf_sa >= 0;
-    if (has_sa) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) plain(P.pf_sa + c, sac[c]);
-    }
-    field_stencil<V, false>(smem, sm + 6 * field_rows, s0 + 6 * field_rows, sp + 6 * field_rows,
-                            N, L, lapX, cX, nofaces);
-    ColorAcc A[V];
-    {
-      Vec<V> cr[3], ci[3];
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        cr[c] = lds<V>(smem, s0 + c * field_rows + (L.r + 1) * N + L.k0);
-        ci[c] = lds<V>(smem, s0 + (3 + c) * field_rows + (L.r + 1) * N + L.k0);
-      }
-#pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
-        const float pic[3] = {ci[0].v[e], ci[1].v[e], ci[2].v[e]};
-        color_begin(A[e], cX[e], mask[e], prc, pic, a.c);
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float lapR[V], cR[V], lapI[V], cI[V];
-      Faces fR[V], fI[V];
-      field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
-                             N, L, lapR, cR, fR);
-      field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
-                             sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
-      float o_r[V], o_i[V], o_rp[V], o_ip[V];
-#pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const ColorCompOut o =
-            color_component(A[e], c, lapR[e], cR[e], rpc[c][e], fR[e], lapI[e], cI[e], ipc[c][e],
-                            fI[e], a.c);
-        o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
-      }
-      stg<V>(a.pr_out + c * n3 + gofs, o_r);
-      stg<V>(a.pi_out + c * n3 + gofs, o_i);
-      if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
-      if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
-    }
-    float sa[V][3];
-    if (has_sa) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        float t[V];
-#pragma unroll
-        for (int e = 0; e < V; ++e) t[e] = sac[c][e];
-#pragma unroll
-        for (int e = 0; e < V; ++e) sa[e][c] = t[e];
-        if (a.sa_clip_out) {
-#pragma unroll
-          for (int e = 0; e < V; ++e) t[e] = fmaxf(t[e], 0.0f);
-          stg<V>(a.sa_clip_out + c * n3 + gofs, t);
-        }
-      }
-    }
-    float o_c[V];
-#pragma unroll
-    for (int e = 0; e < V; ++e) o_c[e] = color_finish(A[e], lapX[e], xp[e], has_sa, sa[e], a.c);
-    stg<V>(a.chi_out + gofs, o_c);
-    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
+  for (int c = 0; c < 3; ++c) {
+    prev(c, rpc[c]);
+    prev(3 + c, ipc[c]);
   }
+  const bool has_sa = P.pf_sa >= 0;
+  if (has_sa) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) plain(P.pf_sa + c, sac[c]);
+  }
+  field_stencil<V, false>(smem, sm + 6 * field_rows, s0 + 6 * field_rows, sp + 6 * field_rows,
+                          N, L, lapX, cX, nofaces);
+  ColorAcc A[V];
+  {
+    Vec<V> cr[3], ci[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cr[c] = lds<V>(smem, s0 + c * field_rows + (L.r + 1) * N + L.k0);
+      ci[c] = lds<V>(smem, s0 + (3 + c) * field_rows + (L.r + 1) * N + L.k0);
+    }
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
+      const float pic[3] = {ci[0].v[e], ci[1].v[e], ci[2].v[e]};
+      color_begin(A[e], cX[e], mask[e], prc, pic, a.c);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float lapR[V], cR[V], lapI[V], cI[V];
+    Faces fR[V], fI[V];
+    field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
+                           N, L, lapR, cR, fR);
+    field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
+                           sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
+    float o_r[V], o_i[V], o_rp[V], o_ip[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const ColorCompOut o =
+          color_component(A[e], c, lapR[e], cR[e], rpc[c][e], fR[e], lapI[e], cI[e], ipc[c][e],
+                          fI[e], a.c);
+      o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
+    }
+    stg<V>(a.pr_out + c * n3 + gofs, o_r);
+    stg<V>(a.pi_out + c * n3 + gofs, o_i);
+    if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
+    if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
+  }
+  float sa[V][3];
+  if (has_sa) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      float t[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) t[e] = sac[c][e];
+#pragma unroll
+      for (int e = 0; e < V; ++e) sa[e][c] = t[e];
+      if (a.sa_clip_out) {
+#pragma unroll
+        for (int e = 0; e < V; ++e) t[e] = fmaxf(t[e], 0.0f);
+        stg<V>(a.sa_clip_out + c * n3 + gofs, t);
+      }
+    }
+  }
+  float o_c[V];
+#pragma unroll
+  for (int e = 0; e < V; ++e) o_c[e] = color_finish(A[e], lapX[e], xp[e], has_sa, sa[e], a.c);
+  stg<V>(a.chi_out + gofs, o_c);
+  if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
 }
 
 // Copies plane (i0 - 1 + u) into stage u % S: the stencil fields' tile rows
@@ -486,6 +444,7 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
 
 template <int LEVEL, int V>
 __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ TmaParams P) {
+  static_assert(LEVEL == LFM_COLOR, "REAL and COMPLEX run on the register-queue kernel");
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
   __shared__ int abort_flag;
@@ -533,7 +492,7 @@ __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ T
       atomicOr(P.a.status, LFM_ERR_DEVICE_TIMEOUT);
     } else {
       const int sf = P.stage_floats;
-      compute_plane<LEVEL, V>(P, smem, (c % S) * sf, ((c + 1) % S) * sf, ((c + 2) % S) * sf,
+      color_plane<V>(P, smem, (c % S) * sf, ((c + 1) % S) * sf, ((c + 2) % S) * sf,
                               i0 + c, L, j);
     }
     __syncthreads();
