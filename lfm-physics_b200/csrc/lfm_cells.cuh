@@ -113,119 +113,142 @@ __device__ __forceinline__ ComplexOutT<T> complex_cell(T lapR, T pr, T pr_prev,
 
 // ---- COLOR (numpy_backend.py:207-382), three colours ----------------------
 // The colour step is split so a kernel can stream one colour at a time:
-// color_begin -> color_component (a = 0, 1, 2) -> color_finish.
-struct ColorAcc {
-  float chi, chi_sq, mask, absorb;
-  float pr_avg, pi_avg;
-  float psi_sq_total, j_total;
-  float ea[3];
-  float jd[3][3];  // per colour, per axis current (for CCV)
+// color_begin -> color_component (a = 0, 1, 2) -> color_finish.  T = float
+// for one cell or F2 for two cells packed; the operations that have no
+// packed form (the division by 3, the float64 step of f_c, the S_a clip)
+// run per lane.
+template <class T>
+struct ColorAccT {
+  T chi, chi_sq, mask, absorb;
+  T pr_avg, pi_avg;
+  T psi_sq_total, j_total;
+  T ea[3];
+  T jd[3][3];  // per colour, per axis current (for CCV)
 };
+using ColorAcc = ColorAccT<float>;
 
-__device__ __forceinline__ void color_begin(ColorAcc& A, float chi, float mask,
-                                            const float pr_c[3], const float pi_c[3],
-                                            const StepConsts& s) {
+__device__ __forceinline__ float div3(float x) { return __fdiv_rn(x, 3.0f); }
+__device__ __forceinline__ F2 div3(F2 x) { return pk(div3(x.v.x), div3(x.v.y)); }
+
+// np.clip(sa, 0, None) as the kernels have always evaluated it
+__device__ __forceinline__ float clip0(float x) { return fmaxf(x, 0.0f); }
+__device__ __forceinline__ F2 clip0(F2 x) { return pk(clip0(x.v.x), clip0(x.v.y)); }
+
+// f_c = sum_sq / total_sq - 1/3 where total_sq > 1e-30, else 0: a float32
+// quotient, then "- 1/3" in float64 (the float64 out array of np.divide),
+// rounded back to float32.
+__device__ __forceinline__ float fc_value(float ssq, float tsq) {
+  const bool safe = tsq > (float)1e-30;
+  const double ratio = safe ? (double)__fdiv_rn(ssq, tsq) : 0.0;
+  return __double2float_rn(__dmul_rn(__dsub_rn(ratio, 1.0 / 3.0), safe ? 1.0 : 0.0));
+}
+__device__ __forceinline__ F2 fc_value(F2 ssq, F2 tsq) {
+  return pk(fc_value(ssq.v.x, tsq.v.x), fc_value(ssq.v.y, tsq.v.y));
+}
+
+template <class T>
+__device__ __forceinline__ void color_begin(ColorAccT<T>& A, T chi, T mask, const T pr_c[3],
+                                            const T pi_c[3], const StepConsts& s) {
   A.chi = chi;
   A.chi_sq = fmul(chi, chi);
   A.mask = mask;
-  A.absorb = fsub(1.0f, mask);
-  A.pr_avg = 0.0f;
-  A.pi_avg = 0.0f;
+  A.absorb = fsub(cst<T>(1.0f), mask);
+  A.pr_avg = cst<T>(0.0f);
+  A.pi_avg = cst<T>(0.0f);
   if (s.use_cc) {  // Pr_avg = (0 + Pr_0 + Pr_1 + Pr_2) / 3   (numpy_backend.py:254-262)
-    float r = 0.0f, i = 0.0f;
+    T r = cst<T>(0.0f), i = cst<T>(0.0f);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       r = fadd(r, pr_c[a]);
       i = fadd(i, pi_c[a]);
     }
-    A.pr_avg = __fdiv_rn(r, 3.0f);
-    A.pi_avg = __fdiv_rn(i, 3.0f);
+    A.pr_avg = div3(r);
+    A.pi_avg = div3(i);
   }
-  A.psi_sq_total = 0.0f;
-  A.j_total = 0.0f;
+  A.psi_sq_total = cst<T>(0.0f);
+  A.j_total = cst<T>(0.0f);
 }
 
-struct ColorCompOut {
-  float pr, pr_prev, pi, pi_prev;
+template <class T>
+struct ColorCompOutT {
+  T pr, pr_prev, pi, pi_prev;
 };
+using ColorCompOut = ColorCompOutT<float>;
 
 // numpy_backend.py:268-310 for colour a.
-__device__ __forceinline__ ColorCompOut color_component(ColorAcc& A, int a, float lapR, float pr,
-                                                        float pr_prev, const Faces& R,
-                                                        float lapI, float pi, float pi_prev,
-                                                        const Faces& I, const StepConsts& s) {
-  float Pr_new = gov01(pr, pr_prev, lapR, A.chi_sq, s);
-  float Pi_new = gov01(pi, pi_prev, lapI, A.chi_sq, s);
+template <class T>
+__device__ __forceinline__ ColorCompOutT<T> color_component(ColorAccT<T>& A, int a, T lapR, T pr,
+                                                            T pr_prev, const FacesT<T>& R, T lapI,
+                                                            T pi, T pi_prev, const FacesT<T>& I,
+                                                            const StepConsts& s) {
+  T Pr_new = gov01(pr, pr_prev, lapR, A.chi_sq, s);
+  T Pi_new = gov01(pi, pi_prev, lapI, A.chi_sq, s);
   if (s.use_cc) {  // -= dt2*eps_cc*chi^2*(Psi_a - Psi_bar)
-    const float t = fmul(s.dt2_eps_cc, A.chi_sq);
+    const T t = pmul(cst<T>(s.dt2_eps_cc), A.chi_sq);  // feeds only the products below
     Pr_new = fsub(Pr_new, fmul(t, fsub(pr, A.pr_avg)));
     Pi_new = fsub(Pi_new, fmul(t, fsub(pi, A.pi_avg)));
   }
-  const float e = fadd(fmul(pr, pr), fmul(pi, pi));
+  const T e = fadd(fmul(pr, pr), fmul(pi, pi));
   A.ea[a] = e;
   A.psi_sq_total = fadd(A.psi_sq_total, e);
-  const float jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
-  const float jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
-  const float jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
-  A.j_total = fadd(A.j_total, fmul(0.5f, fadd(fadd(jx, jy), jz)));
+  const T jx = current_axis(pr, pi, R.ip, R.im, I.ip, I.im);
+  const T jy = current_axis(pr, pi, R.jp, R.jm, I.jp, I.jm);
+  const T jz = current_axis(pr, pi, R.kp, R.km, I.kp, I.km);
+  A.j_total = fadd(A.j_total, fmul(cst<T>(0.5f), fadd(fadd(jx, jy), jz)));
   A.jd[a][0] = jx;
   A.jd[a][1] = jy;
   A.jd[a][2] = jz;
-  ColorCompOut o;
-  o.pr = fmul(Pr_new, A.absorb);
-  o.pi = fmul(Pi_new, A.absorb);
-  o.pr_prev = fmul(pr, A.absorb);
-  o.pi_prev = fmul(pi, A.absorb);
+  ColorCompOutT<T> o;  // stored values only
+  o.pr = pmul(Pr_new, A.absorb);
+  o.pi = pmul(Pi_new, A.absorb);
+  o.pr_prev = pmul(pr, A.absorb);
+  o.pi_prev = pmul(pi, A.absorb);
   return o;
 }
 
 // f_c, CCV, SCV and GOV-02 (numpy_backend.py:312-370).  sa_raw holds the
 // unclipped S_a values of the cell (clipped here) or is ignored when
 // has_sa is false.  Returns the new chi.
-__device__ __forceinline__ float color_finish(const ColorAcc& A, float lapX, float chi_prev,
-                                              bool has_sa, const float sa_raw[3],
-                                              const StepConsts& s) {
+template <class T>
+__device__ __forceinline__ T color_finish(const ColorAccT<T>& A, T lapX, T chi_prev, bool has_sa,
+                                          const T sa_raw[3], const StepConsts& s) {
   const float third = (float)(1.0 / 3.0);
-  float color_var = 0.0f;
+  T color_var = cst<T>(0.0f);
   if (s.use_fc) {
-    float ssq = fadd(fmul(A.ea[0], A.ea[0]), fmul(A.ea[1], A.ea[1]));
+    T ssq = fadd(fmul(A.ea[0], A.ea[0]), fmul(A.ea[1], A.ea[1]));
     ssq = fadd(ssq, fmul(A.ea[2], A.ea[2]));
-    const float tsq = fmul(A.psi_sq_total, A.psi_sq_total);
-    const bool safe = tsq > (float)1e-30;
-    // float32 quotient, then "- 1/3" in float64 (the float64 out array of
-    // np.divide), rounded back to float32.
-    const double ratio = safe ? (double)__fdiv_rn(ssq, tsq) : 0.0;
-    const float fc = __double2float_rn(__dmul_rn(__dsub_rn(ratio, 1.0 / 3.0), safe ? 1.0 : 0.0));
-    color_var = fmul(fmul(fmul(s.kc_over_chi0, A.chi), fc), A.psi_sq_total);
+    const T tsq = pmul(A.psi_sq_total, A.psi_sq_total);  // feeds only the comparison and quotient
+    const T fc = fc_value(ssq, tsq);
+    color_var = fmul(pmul(pmul(cst<T>(s.kc_over_chi0), A.chi), fc), A.psi_sq_total);
   }
-  float ccv = 0.0f;
+  T ccv = cst<T>(0.0f);
   if (s.use_ccv) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      float sq = fadd(fmul(A.jd[0][d], A.jd[0][d]), fmul(A.jd[1][d], A.jd[1][d]));
+      T sq = fadd(fmul(A.jd[0][d], A.jd[0][d]), fmul(A.jd[1][d], A.jd[1][d]));
       sq = fadd(sq, fmul(A.jd[2][d], A.jd[2][d]));
-      float sm = fadd(A.jd[0][d], A.jd[1][d]);
+      T sm = fadd(A.jd[0][d], A.jd[1][d]);
       sm = fadd(sm, A.jd[2][d]);
-      ccv = fadd(ccv, fsub(sq, fmul(third, fmul(sm, sm))));
+      ccv = fadd(ccv, fsub(sq, fmul(cst<T>(third), pmul(sm, sm))));
     }
   }
-  float scv = 0.0f;
+  T scv = cst<T>(0.0f);
   if (has_sa) {
-    float ssum = 0.0f, ssq = 0.0f;
+    T ssum = cst<T>(0.0f), ssq = cst<T>(0.0f);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float v = fmaxf(sa_raw[a], 0.0f);  // np.clip(sa, 0, None)
+      const T v = clip0(sa_raw[a]);
       ssum = fadd(ssum, v);
       ssq = fadd(ssq, fmul(v, v));
     }
-    scv = fsub(ssq, fmul(third, fmul(ssum, ssum)));
+    scv = fsub(ssq, fmul(cst<T>(third), pmul(ssum, ssum)));
   }
-  const float src =
-      fmul(fmul(s.k_over_chi0, A.chi), fsub(fadd(A.psi_sq_total, fmul(s.eps_w, A.j_total)), s.e0_sq));
-  float acc = fsub(lapX, src);
+  const T src = fmul(pmul(cst<T>(s.k_over_chi0), A.chi),
+                     fsub(fadd(A.psi_sq_total, fmul(cst<T>(s.eps_w), A.j_total)), cst<T>(s.e0_sq)));
+  T acc = fsub(lapX, src);
   acc = fsub(acc, color_var);
-  acc = fsub(acc, fmul(s.kappa_string, ccv));
-  acc = fsub(acc, fmul(s.kappa_tube, scv));
+  acc = fsub(acc, fmul(cst<T>(s.kappa_string), ccv));
+  acc = fsub(acc, fmul(cst<T>(s.kappa_tube), scv));
   acc = mexican_hat(acc, A.chi, A.chi_sq, s);
   return gov02_finish(A.chi, chi_prev, acc, A.mask, A.absorb, s);
 }

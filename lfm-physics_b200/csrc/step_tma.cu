@@ -261,9 +261,10 @@ __device__ __forceinline__ void field_stencil(const float* smem, int fm, int f0,
   const float M_0_r = right_nb(M_0.v[0], smem, fm + r0, L);
   const float P_0_l = left_nb(P_0.v[V - 1], smem, fp + r0, L);
   const float P_0_r = right_nb(P_0.v[0], smem, fp + r0, L);
+  S19 st[V];
 #pragma unroll
   for (int e = 0; e < V; ++e) {
-    S19 s;
+    S19& s = st[e];
     s.c = A_0.v[e];
     s.im = M_0.v[e];
     s.ip = P_0.v[e];
@@ -283,13 +284,18 @@ __device__ __forceinline__ void field_stencil(const float* smem, int fm, int f0,
     s.jmkp = e < V - 1 ? A_m.v[e + 1] : A_m_r;
     s.jpkm = e > 0 ? A_p.v[e - 1] : A_p_l;
     s.jpkp = e < V - 1 ? A_p.v[e + 1] : A_p_r;
-    lap[e] = lap19(s);
+    if constexpr (V != 2) lap[e] = lap19(s);
     ctr[e] = s.c;
     if (FACES) {
       faces[e].im = s.im; faces[e].ip = s.ip;
       faces[e].jm = s.jm; faces[e].jp = s.jp;
       faces[e].km = s.km; faces[e].kp = s.kp;
     }
+  }
+  if constexpr (V == 2) {  // i/j sums of both cells as packed additions
+    const F2 l = lap19_pair(st[0], st[1]);
+    lap[0] = l.v.x;
+    lap[1] = l.v.y;
   }
 }
 
@@ -348,14 +354,63 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
   }
   field_stencil<V, false>(smem, sm + 6 * field_rows, s0 + 6 * field_rows, sp + 6 * field_rows,
                           N, L, lapX, cX, nofaces);
-  ColorAcc A[V];
-  {
-    Vec<V> cr[3], ci[3];
+  Vec<V> cr[3], ci[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    cr[c] = lds<V>(smem, s0 + c * field_rows + (L.r + 1) * N + L.k0);
+    ci[c] = lds<V>(smem, s0 + (3 + c) * field_rows + (L.r + 1) * N + L.k0);
+  }
+  if constexpr (V == 2) {
+    // both cells of the lane at once: packed additions, per lane where needed
+    const F2 prc[3] = {pk(cr[0].v[0], cr[0].v[1]), pk(cr[1].v[0], cr[1].v[1]),
+                       pk(cr[2].v[0], cr[2].v[1])};
+    const F2 pic[3] = {pk(ci[0].v[0], ci[0].v[1]), pk(ci[1].v[0], ci[1].v[1]),
+                       pk(ci[2].v[0], ci[2].v[1])};
+    ColorAccT<F2> A;
+    color_begin(A, pk(cX[0], cX[1]), pk(mask[0], mask[1]), prc, pic, a.c);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      cr[c] = lds<V>(smem, s0 + c * field_rows + (L.r + 1) * N + L.k0);
-      ci[c] = lds<V>(smem, s0 + (3 + c) * field_rows + (L.r + 1) * N + L.k0);
+      float lapR[V], cR[V], lapI[V], cI[V];
+      Faces fR[V], fI[V];
+      field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows,
+                             sp + c * field_rows, N, L, lapR, cR, fR);
+      field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
+                             sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
+      const ColorCompOutT<F2> o = color_component(
+          A, c, pk(lapR[0], lapR[1]), pk(cR[0], cR[1]), pk(rpc[c][0], rpc[c][1]),
+          pk_faces(fR[0], fR[1]), pk(lapI[0], lapI[1]), pk(cI[0], cI[1]),
+          pk(ipc[c][0], ipc[c][1]), pk_faces(fI[0], fI[1]), a.c);
+      const float o_r[V] = {o.pr.v.x, o.pr.v.y}, o_i[V] = {o.pi.v.x, o.pi.v.y};
+      stg<V>(a.pr_out + c * n3 + gofs, o_r);
+      stg<V>(a.pi_out + c * n3 + gofs, o_i);
+      if (a.pr_prev_out) {
+        const float o_rp[V] = {o.pr_prev.v.x, o.pr_prev.v.y};
+        stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
+      }
+      if (a.pi_prev_out) {
+        const float o_ip[V] = {o.pi_prev.v.x, o.pi_prev.v.y};
+        stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
+      }
     }
+    F2 saf[3];
+    if (has_sa) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        saf[c] = pk(sac[c][0], sac[c][1]);
+        if (a.sa_clip_out) {
+          const float t[V] = {fmaxf(sac[c][0], 0.0f), fmaxf(sac[c][1], 0.0f)};
+          stg<V>(a.sa_clip_out + c * n3 + gofs, t);
+        }
+      }
+    }
+    const F2 oc = color_finish(A, pk(lapX[0], lapX[1]), pk(xp[0], xp[1]), has_sa, saf, a.c);
+    const float o_c[V] = {oc.v.x, oc.v.y};
+    stg<V>(a.chi_out + gofs, o_c);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
+    return;
+  }
+  ColorAcc A[V];
+  {
 #pragma unroll
     for (int e = 0; e < V; ++e) {
       const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
