@@ -251,16 +251,34 @@ __device__ __forceinline__ void field_stencil(const float* smem, int fm, int f0,
   const Vec<V> P_m = lds<V>(smem, fp + rm + L.k0);
   const Vec<V> P_0 = lds<V>(smem, fp + r0 + L.k0);
   const Vec<V> P_p = lds<V>(smem, fp + rp + L.k0);
-  const float A_m_l = left_nb(A_m.v[V - 1], smem, f0 + rm, L);
-  const float A_m_r = right_nb(A_m.v[0], smem, f0 + rm, L);
-  const float A_0_l = left_nb(A_0.v[V - 1], smem, f0 + r0, L);
-  const float A_0_r = right_nb(A_0.v[0], smem, f0 + r0, L);
-  const float A_p_l = left_nb(A_p.v[V - 1], smem, f0 + rp, L);
-  const float A_p_r = right_nb(A_p.v[0], smem, f0 + rp, L);
-  const float M_0_l = left_nb(M_0.v[V - 1], smem, fm + r0, L);
-  const float M_0_r = right_nb(M_0.v[0], smem, fm + r0, L);
-  const float P_0_l = left_nb(P_0.v[V - 1], smem, fp + r0, L);
-  const float P_0_r = right_nb(P_0.v[0], smem, fp + r0, L);
+  // k0-1 and k0+V: with two cells per lane, the second and first value of the
+  // aligned neighbouring pairs (periodic in k); otherwise the adjacent lanes'
+  // values by shuffle, from shared memory at row ends and warp edges.
+  float A_m_l, A_m_r, A_0_l, A_0_r, A_p_l, A_p_r, M_0_l, M_0_r, P_0_l, P_0_r;
+  if constexpr (V == 2) {
+    const int kl = L.km1 - 1, kr = L.kpv;
+    A_m_l = lds<2>(smem, f0 + rm + kl).v[1];
+    A_m_r = lds<2>(smem, f0 + rm + kr).v[0];
+    A_0_l = lds<2>(smem, f0 + r0 + kl).v[1];
+    A_0_r = lds<2>(smem, f0 + r0 + kr).v[0];
+    A_p_l = lds<2>(smem, f0 + rp + kl).v[1];
+    A_p_r = lds<2>(smem, f0 + rp + kr).v[0];
+    M_0_l = lds<2>(smem, fm + r0 + kl).v[1];
+    M_0_r = lds<2>(smem, fm + r0 + kr).v[0];
+    P_0_l = lds<2>(smem, fp + r0 + kl).v[1];
+    P_0_r = lds<2>(smem, fp + r0 + kr).v[0];
+  } else {
+    A_m_l = left_nb(A_m.v[V - 1], smem, f0 + rm, L);
+    A_m_r = right_nb(A_m.v[0], smem, f0 + rm, L);
+    A_0_l = left_nb(A_0.v[V - 1], smem, f0 + r0, L);
+    A_0_r = right_nb(A_0.v[0], smem, f0 + r0, L);
+    A_p_l = left_nb(A_p.v[V - 1], smem, f0 + rp, L);
+    A_p_r = right_nb(A_p.v[0], smem, f0 + rp, L);
+    M_0_l = left_nb(M_0.v[V - 1], smem, fm + r0, L);
+    M_0_r = right_nb(M_0.v[0], smem, fm + r0, L);
+    P_0_l = left_nb(P_0.v[V - 1], smem, fp + r0, L);
+    P_0_r = right_nb(P_0.v[0], smem, fp + r0, L);
+  }
   S19 st[V];
 #pragma unroll
   for (int e = 0; e < V; ++e) {
@@ -407,59 +425,59 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
     const float o_c[V] = {oc.v.x, oc.v.y};
     stg<V>(a.chi_out + gofs, o_c);
     if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
-    return;
-  }
-  ColorAcc A[V];
-  {
+  } else {  // one cell per lane
+    ColorAcc A[V];
+    {
 #pragma unroll
-    for (int e = 0; e < V; ++e) {
-      const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
-      const float pic[3] = {ci[0].v[e], ci[1].v[e], ci[2].v[e]};
-      color_begin(A[e], cX[e], mask[e], prc, pic, a.c);
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    float lapR[V], cR[V], lapI[V], cI[V];
-    Faces fR[V], fI[V];
-    field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
-                           N, L, lapR, cR, fR);
-    field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
-                           sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
-    float o_r[V], o_i[V], o_rp[V], o_ip[V];
-#pragma unroll
-    for (int e = 0; e < V; ++e) {
-      const ColorCompOut o =
-          color_component(A[e], c, lapR[e], cR[e], rpc[c][e], fR[e], lapI[e], cI[e], ipc[c][e],
-                          fI[e], a.c);
-      o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
-    }
-    stg<V>(a.pr_out + c * n3 + gofs, o_r);
-    stg<V>(a.pi_out + c * n3 + gofs, o_i);
-    if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
-    if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
-  }
-  float sa[V][3];
-  if (has_sa) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      float t[V];
-#pragma unroll
-      for (int e = 0; e < V; ++e) t[e] = sac[c][e];
-#pragma unroll
-      for (int e = 0; e < V; ++e) sa[e][c] = t[e];
-      if (a.sa_clip_out) {
-#pragma unroll
-        for (int e = 0; e < V; ++e) t[e] = fmaxf(t[e], 0.0f);
-        stg<V>(a.sa_clip_out + c * n3 + gofs, t);
+      for (int e = 0; e < V; ++e) {
+        const float prc[3] = {cr[0].v[e], cr[1].v[e], cr[2].v[e]};
+        const float pic[3] = {ci[0].v[e], ci[1].v[e], ci[2].v[e]};
+        color_begin(A[e], cX[e], mask[e], prc, pic, a.c);
       }
     }
-  }
-  float o_c[V];
 #pragma unroll
-  for (int e = 0; e < V; ++e) o_c[e] = color_finish(A[e], lapX[e], xp[e], has_sa, sa[e], a.c);
-  stg<V>(a.chi_out + gofs, o_c);
-  if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
+    for (int c = 0; c < 3; ++c) {
+      float lapR[V], cR[V], lapI[V], cI[V];
+      Faces fR[V], fI[V];
+      field_stencil<V, true>(smem, sm + c * field_rows, s0 + c * field_rows, sp + c * field_rows,
+                             N, L, lapR, cR, fR);
+      field_stencil<V, true>(smem, sm + (3 + c) * field_rows, s0 + (3 + c) * field_rows,
+                             sp + (3 + c) * field_rows, N, L, lapI, cI, fI);
+      float o_r[V], o_i[V], o_rp[V], o_ip[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const ColorCompOut o =
+            color_component(A[e], c, lapR[e], cR[e], rpc[c][e], fR[e], lapI[e], cI[e], ipc[c][e],
+                            fI[e], a.c);
+        o_r[e] = o.pr; o_i[e] = o.pi; o_rp[e] = o.pr_prev; o_ip[e] = o.pi_prev;
+      }
+      stg<V>(a.pr_out + c * n3 + gofs, o_r);
+      stg<V>(a.pi_out + c * n3 + gofs, o_i);
+      if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
+      if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
+    }
+    float sa[V][3];
+    if (has_sa) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float t[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) t[e] = sac[c][e];
+#pragma unroll
+        for (int e = 0; e < V; ++e) sa[e][c] = t[e];
+        if (a.sa_clip_out) {
+#pragma unroll
+          for (int e = 0; e < V; ++e) t[e] = fmaxf(t[e], 0.0f);
+          stg<V>(a.sa_clip_out + c * n3 + gofs, t);
+        }
+      }
+    }
+    float o_c[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) o_c[e] = color_finish(A[e], lapX[e], xp[e], has_sa, sa[e], a.c);
+    stg<V>(a.chi_out + gofs, o_c);
+    if (a.chi_prev_out) stg<V>(a.chi_prev_out + gofs, cX);
+  }
 }
 
 // Copies plane (i0 - 1 + u) into stage u % S: the stencil fields' tile rows
