@@ -118,6 +118,39 @@ def test_protocol_step_color_bit_exact(be, path, N, couplings):
         assert bits_equal(be.to_numpy(d), r), f"output {k}"
 
 
+@pytest.mark.parametrize("N", [64, 128])
+def test_color_fused_default_tile_bit_exact(be, N):
+    """The COLOR kernel on the planner's own tiles at larger N (4-row tiles, deep
+    rings, point fields from global memory, packed cell math): a few resident steps
+    with every coupling but S_a against the oracle, then one protocol step."""
+    from lfm_b200 import Evolver, _lib
+
+    cfg = _parity_config("color", sa=False, N=N)
+    rng = np.random.default_rng(400 + N)
+    pr = (0.5 * rng.standard_normal((3, N, N, N))).astype(np.float32)
+    pi = (0.5 * rng.standard_normal((3, N, N, N))).astype(np.float32)
+    chi = (CHI0 + 0.01 * rng.standard_normal((N, N, N))).astype(np.float32)
+    _lib.set_step_path(_lib.PATH_FUSED)
+    try:
+        ev = Evolver(cfg, backend=be)
+        lat = O.OracleLattice(cfg)
+        for t in (ev, lat):
+            t.set_psi_real(pr)
+            t.set_psi_imag(pi)
+            t.set_chi(chi)
+        ev.evolve(3)
+        O.set_threads(O.max_threads())
+        lat.step(3)
+        used = _lib.tune_get(2, N)
+        assert used["vec"] == 2 and used["tj"] >= 2, used
+        assert bits_equal(ev.get_psi_real().ravel(), lat.pr)
+        assert bits_equal(ev.get_psi_imag().ravel(), lat.pi)
+        assert bits_equal(ev.get_chi().ravel(), lat.chi)
+        assert bits_equal(ev.get_psi_real_prev().ravel(), lat.prp)
+    finally:
+        _lib.set_step_path(_lib.PATH_AUTO)
+
+
 @pytest.mark.parametrize("N,tj", [(16, 4), (32, 2), (64, 2)])
 def test_color_one_cell_per_lane_bit_exact(be, N, tj):
     """The COLOR kernel with one cell per lane (a tuning option), on the streamed
