@@ -483,8 +483,12 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
 // Copies plane (i0 - 1 + u) into stage u % S: the stencil fields' tile rows
 // and halo rows, and with PT the point fields' tile rows (the register-queue
 // kernels read them from the stage; the barrier kernel reads them from global
-// memory).
-template <bool SLAB = true, bool PT = true>
+// memory).  ONE: away from the wrap in j, a stencil field's rows j0-1 ..
+// j0+TJ are contiguous and go as one copy instead of the tile rows and two
+// one-row halo copies.  Measured with identical bits: COMPLEX +4 % at 256^3
+// and 512^3, the compensated REAL step +1.5 %; the plain REAL step -0.5 % and
+// the COLOR stencil -3.6 %, so those keep the separate halo copies.
+template <bool SLAB = true, bool PT = true, bool ONE = false>
 __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                             int u, int i0, int i1, int j0) {
   const int N = P.N, TJ = P.TJ;
@@ -500,12 +504,17 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
   const int jm = (j0 == 0) ? N - 1 : j0 - 1;
   const int jp = (j0 + TJ == N) ? 0 : j0 + TJ;
   const int64_t plane = (int64_t)pw * N;
+  const bool contiguous = ONE && j0 > 0 && j0 + TJ < N;
   for (int f = 0; f < P.ns; ++f) {
     float* d = st + (size_t)f * (TJ + 2) * N;
     const float* g = P.sf[f];
-    bulk_copy_g2s(d + N, g + (plane + j0) * N, row_bytes * TJ, &bars[s]);
-    bulk_copy_g2s(d, g + (plane + jm) * N, row_bytes, &bars[s]);
-    bulk_copy_g2s(d + (size_t)(TJ + 1) * N, g + (plane + jp) * N, row_bytes, &bars[s]);
+    if (contiguous) {
+      bulk_copy_g2s(d, g + (plane + j0 - 1) * N, row_bytes * (TJ + 2), &bars[s]);
+    } else {
+      bulk_copy_g2s(d + N, g + (plane + j0) * N, row_bytes * TJ, &bars[s]);
+      bulk_copy_g2s(d, g + (plane + jm) * N, row_bytes, &bars[s]);
+      bulk_copy_g2s(d + (size_t)(TJ + 1) * N, g + (plane + jp) * N, row_bytes, &bars[s]);
+    }
   }
   if (point) {
     float* base = st + (size_t)P.ns * (TJ + 2) * N;
@@ -514,6 +523,10 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
                     &bars[s]);
   }
 }
+
+// The register-queue kernels that copy a stencil field's rows as one (above).
+template <int LEVEL, bool COMP>
+constexpr bool kOneCopy = LEVEL == LFM_COMPLEX || COMP;
 
 template <int LEVEL, int V>
 __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ TmaParams P) {
@@ -973,7 +986,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       sh.done[s_cur] = 0u;
       fence_proxy_async_smem();
       if (c + 1 + g.S < nplanes) {
-        issue_plane<G::kSlab>(P, smem, bars, c + 1 + g.S, i0, i1, j0);
+        issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, c + 1 + g.S, i0, i1, j0);
         atomicMax(&sh.issued, c + 2 + g.S);
       }
     }
@@ -1052,7 +1065,8 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
       bulk_copy_g2s(smem + tab_at + 1, P.a.lut.table, 4u * (uint32_t)tab_bulk, &bars[0]);
     }
     const int first = min(S, nplanes);
-    for (int u = 0; u < first; ++u) issue_plane<G::kSlab>(P, smem, bars, u, i0, i1, j0);
+    for (int u = 0; u < first; ++u)
+      issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, u, i0, i1, j0);
     sh.issued = first;
   }
   if (tab_at >= 0) {
@@ -1083,7 +1097,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     // stage 0 (plane i0-1) is dead: refill it with u = S
     if (tid == 0 && S < nplanes) {
       fence_proxy_async_smem();
-      issue_plane<G::kSlab>(P, smem, bars, S, i0, i1, j0);
+      issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, S, i0, i1, j0);
       sh.issued = S + 1;
     }
     int s_cur = 1 % S, s_nxt = 2 % S;
