@@ -390,6 +390,12 @@ int lfm_tune_get(int level, int N, int* vec, int* tj, int* stages, int* ic, int*
  * device-side waits set on timeout; synchronises the current device. */
 int lfm_device_status(int* status_out, int clear);
 
+/* Failure-detection test: launches, on `stream`, one CTA that waits through
+ * the step kernels' bounded wait on an mbarrier nothing completes.  The wait
+ * gives up after limit_ns (1 us .. 1 s), ORs LFM_ERR_DEVICE_TIMEOUT into the
+ * device status word and returns; the context stays usable. */
+int lfm_selftest_device_timeout(unsigned long long limit_ns, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

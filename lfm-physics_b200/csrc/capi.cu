@@ -1246,6 +1246,17 @@ int lfm_batch_destroy(lfm_batch* batch) {
   return LFM_OK;
 }
 
+int lfm_selftest_device_timeout(unsigned long long limit_ns, void* stream) {
+  if (limit_ns < 1000ull || limit_ns > 1000000000ull)
+    return fail(LFM_ERR_INVALID_ARG, "limit %llu ns not in [1 us, 1 s]", limit_ns);
+  int* status = nullptr;
+  int rc = status_word(&status);
+  if (rc != LFM_OK) return rc;
+  cudaError_t e = lfm::launch_wait_selftest(status, limit_ns, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "wait self-test launch");
+  return LFM_OK;
+}
+
 int lfm_device_status(int* status_out, int clear) {
   if (!status_out) return fail(LFM_ERR_INVALID_ARG, "null output");
   int v = 0;

@@ -49,6 +49,9 @@ cudaError_t launch_direct_step(const StepArgs& a, cudaStream_t stream);
 // size has no tile configuration, so the caller can take the direct path.
 cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream);
 
+// A bounded wait that must give up (failure-detection test, step_tma.cu).
+cudaError_t launch_wait_selftest(int* status, uint64_t limit_ns, cudaStream_t stream);
+
 // S_a pipeline pieces (helmholtz.cu).
 cudaError_t launch_color_energy(const float* pr, const float* pi, float* e, int N,
                                 cudaStream_t stream);

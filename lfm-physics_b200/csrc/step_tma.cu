@@ -1540,6 +1540,28 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 }  // namespace
 
+namespace {
+
+// One CTA waits on an mbarrier that nothing arrives at, through the bounded
+// wait of the step kernels: the wait gives up after limit_ns and records
+// LFM_ERR_DEVICE_TIMEOUT in the status word, and the kernel returns.
+__global__ void wait_selftest_kernel(int* status, uint64_t limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0u, limit_ns)) atomicOr(status, LFM_ERR_DEVICE_TIMEOUT);
+}
+
+}  // namespace
+
+cudaError_t launch_wait_selftest(int* status, uint64_t limit_ns, cudaStream_t stream) {
+  wait_selftest_kernel<<<1, 32, 0, stream>>>(status, limit_ns);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   const int N = a.N;
   if (N % 4 != 0 || N < 8) return cudaErrorNotSupported;

@@ -96,6 +96,7 @@ _SIGNATURES = {
                        c_int, POINTER(c_int), POINTER(c_int32)],
     "lfm_tune_set": [c_int] * 6,
     "lfm_tune_get": [c_int, c_int] + [POINTER(c_int)] * 6,
+    "lfm_selftest_device_timeout": [ctypes.c_ulonglong, _P],
 }
 
 _lib = None
