@@ -127,7 +127,8 @@ lfm::MaskLut device_lut(const float* table, const lfm_mask_lut* lut) {
 
 int check_lut(const float* table, const lfm_mask_lut* lut, int N) {
   if (!lut) return fail(LFM_ERR_INVALID_ARG, "mask lookup table descriptor is null");
-  if (lut->N != N) return fail(LFM_ERR_INVALID_ARG, "lookup table is for N=%d, step N=%d", lut->N, N);
+  if (lut->N != N)
+    return fail(LFM_ERR_INVALID_ARG, "lookup table is for N=%d, step N=%d", lut->N, N);
   if (lut->count > 0 && !table) return fail(LFM_ERR_INVALID_ARG, "mask table pointer is null");
   if (lut->shift != (N % 2 == 0 ? 3 : 2))
     return fail(LFM_ERR_INVALID_ARG, "mask table shift %d does not match N=%d", lut->shift, N);
@@ -974,7 +975,8 @@ int validate_batch_tuning(const lfm_batch_tuning* in, lfm_batch_tuning* t) {
   }
   if (t->threads < 32 || t->threads > 512 || t->threads % 32)
     return fail(LFM_ERR_INVALID_ARG, "threads %d not a multiple of 32 in [32, 512]", t->threads);
-  if (t->stages < 3 || t->stages > 6) return fail(LFM_ERR_INVALID_ARG, "stages %d not in [3, 6]", t->stages);
+  if (t->stages < 3 || t->stages > 6)
+    return fail(LFM_ERR_INVALID_ARG, "stages %d not in [3, 6]", t->stages);
   if (t->item_cells < 1024) return fail(LFM_ERR_INVALID_ARG, "item_cells %d < 1024", t->item_cells);
   if (t->ctas_per_sm < 0) return fail(LFM_ERR_INVALID_ARG, "ctas_per_sm %d", t->ctas_per_sm);
   return LFM_OK;
@@ -1104,7 +1106,8 @@ int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_
   const int total = (int)plan.items.size();
   if (nitems_out) *nitems_out = total;
   if (items_out) {
-    if (max_items < total) return fail(LFM_ERR_CAPACITY, "%d items > capacity %d", total, max_items);
+    if (max_items < total)
+      return fail(LFM_ERR_CAPACITY, "%d items > capacity %d", total, max_items);
     for (int k = 0; k < total; ++k) {
       const lfm::BatchItem& it = plan.items[k];
       items_out[6 * k + 0] = it.level;

@@ -1240,7 +1240,8 @@ __global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ 
   __shared__ int s_item;
   sh.abort_flag = 0;
   if (B.real_items > 0)
-    batch_level<LFM_REAL, 4, TABM>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P, s_item);
+    batch_level<LFM_REAL, 4, TABM>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P,
+                                   s_item);
   __syncthreads();
   if (!sh.abort_flag && B.nitems > B.real_items)
     batch_level<LFM_COMPLEX, 2, TABM>(B, B.items + B.real_items, B.nitems - B.real_items,
@@ -1280,7 +1281,8 @@ int carveout_kb(int bytes) {
 // when it is staged there); l1_table_bytes: a table read through L1 that the
 // carveout must leave room for (0 when none).
 Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threads,
-              int regs, const TileConfig* forced, int extra_smem, int l1_table_bytes, int planes = 0) {
+              int regs, const TileConfig* forced, int extra_smem, int l1_table_bytes,
+              int planes = 0) {
   if (planes <= 0) planes = N;  // planes the march covers (a slab's own planes)
   Choice best;
   double best_score = -1.0;
@@ -1654,7 +1656,8 @@ cudaError_t grant_smem(K kernel, int smem, int* granted) {
   if (smem <= *granted) return cudaSuccess;
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   cudaFuncAttributes fa{};
   if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
   if (e != cudaSuccess) return e;
