@@ -118,6 +118,41 @@ def test_protocol_step_color_bit_exact(be, path, N, couplings):
         assert bits_equal(be.to_numpy(d), r), f"output {k}"
 
 
+def test_largest_tested_lattice_fused_and_direct_agree(be):
+    """1024^3 REAL, two steps.  The fused kernel (a run-time tile, with the sponge table
+    read through L1 at this size) and the direct kernel share the cell arithmetic but
+    none of the addressing; their states agree bit for bit.  The oracle is too slow at
+    this size; both kernels are held to it bit for bit at the smaller ones."""
+    import torch
+
+    from lfm_b200 import Evolver, _lib
+    from lfm_b200.config import gravity_only
+
+    N = 1024
+    g = torch.Generator(device=be.device).manual_seed(11)
+    E = 0.1 * torch.randn(N**3, device=be.device, generator=g)
+    chi = 19.0 + 1e-3 * torch.rand(N**3, device=be.device, generator=g)
+    states = []
+    try:
+        for path in (_lib.PATH_FUSED, _lib.PATH_DIRECT):
+            _lib.set_step_path(path)
+            ev = Evolver(gravity_only(N), backend=be)
+            ev.set_psi_real(E)
+            ev.set_chi(chi)
+            ev.evolve(2)
+            if path == _lib.PATH_FUSED:
+                assert _lib.tune_get(0, N) is not None
+            states.append([t.clone() for t in (ev._pr[ev._cur], ev._pr[1 - ev._cur],
+                                               ev._chi[ev._cur], ev._chi[1 - ev._cur])])
+            del ev
+            torch.cuda.empty_cache()
+    finally:
+        _lib.set_step_path(_lib.PATH_AUTO)
+    for a, b in zip(*states):
+        assert torch.equal(a, b)
+    assert _lib.device_status() == 0
+
+
 @pytest.mark.parametrize("N", [64, 128])
 def test_color_fused_default_tile_bit_exact(be, N):
     """The COLOR kernel on the planner's own tiles at larger N (4-row tiles, deep
