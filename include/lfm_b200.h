@@ -357,13 +357,17 @@ int lfm_metrics_f64(lfm_context* ctx, int level, const float* psi_r, const float
  * a process whose device memory is held by another allocator (a caching
  * allocator such as PyTorch's can keep the free memory to itself), or a
  * program that must not allocate after start-up -- and that therefore hold
- * no lfm_context.  The per-CTA partials go to a static device array of about
- * 240 KB that every GPU loading the library keeps until the process ends;
- * lattices up to 512^3 cells fit, larger ones return LFM_ERR_CAPACITY.  The
- * first call on each device looks up the array's device address and should
- * come before any stream capture on that device.  All calls share the array:
- * calls that overlap on the GPU (two streams, two threads) race; serialise
- * them.  Same outputs, in the same order, as lfm_metrics_f64. */
+ * no lfm_context.  The per-CTA partials go to a static device array of
+ * 196,704 bytes (192 KiB: 2049 rows of 12 doubles) that every GPU loading
+ * the library keeps until the process ends; lattices up to 512^3 cells fit,
+ * larger ones return LFM_ERR_CAPACITY.  The first call on each device looks
+ * up the array's device address and should come before any stream capture on
+ * that device; the address is the device's primary context's, so calls must
+ * run with the primary context current (the CUDA runtime's default).  All
+ * calls share the array: calls that overlap on the GPU (two streams, two
+ * threads) race; serialise them.  Outputs come in the same order as
+ * lfm_metrics_f64's: chi min/max and the cell counts are identical, and the
+ * sums agree to rounding (the partial sums are grouped differently). */
 int lfm_metrics_f64_noalloc(int level, const float* psi_r, const float* psi_r_prev,
                             const float* psi_i, const float* psi_i_prev, const float* chi, int N,
                             double dt, double c, double boundary_fraction,
@@ -387,7 +391,13 @@ int lfm_tune_get(int level, int N, int* vec, int* tj, int* stages, int* ic, int*
                  int* smem);
 
 /* Reads (and optionally clears) the device status word that bounded
- * device-side waits set on timeout; synchronises the current device. */
+ * device-side waits set on timeout.  It first synchronises the current
+ * device (cudaDeviceSynchronize), so every kernel launched before the call,
+ * on any stream, has finished; with clear, only the bits it read are cleared
+ * (atomically on the device).  A step whose wait gave up has returned with
+ * its outputs partly written, so a non-zero word means the state is not
+ * usable.  The Python layer (Evolver.get_*, synchronize, BatchedLattices and
+ * SlabEvolver reads) calls this and raises LfmError on a non-zero word. */
 int lfm_device_status(int* status_out, int clear);
 
 /* Failure-detection test: launches, on `stream`, one CTA that waits through

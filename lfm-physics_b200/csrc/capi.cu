@@ -24,6 +24,17 @@
 __device__ int g_lfm_status;
 
 namespace {
+__global__ void status_clear_kernel(int bits) { atomicAnd(&g_lfm_status, ~bits); }
+}  // namespace
+
+namespace lfm {
+cudaError_t launch_status_clear(int bits) {
+  status_clear_kernel<<<1, 1>>>(bits);
+  return cudaGetLastError();
+}
+}  // namespace lfm
+
+namespace {
 
 thread_local std::string t_detail;
 
@@ -1262,12 +1273,18 @@ int lfm_selftest_device_timeout(unsigned long long limit_ns, void* stream) {
 
 int lfm_device_status(int* status_out, int clear) {
   if (!status_out) return fail(LFM_ERR_INVALID_ARG, "null output");
+  // Every kernel of this process on the device is finished before the read,
+  // whatever stream (blocking or not) it was launched on.
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceSynchronize");
   int v = 0;
-  cudaError_t e = cudaMemcpyFromSymbol(&v, g_lfm_status, sizeof v);
+  e = cudaMemcpyFromSymbol(&v, g_lfm_status, sizeof v);
   if (e != cudaSuccess) return cuda_fail(e, "read status word");
-  if (clear) {
-    const int zero = 0;
-    e = cudaMemcpyToSymbol(g_lfm_status, &zero, sizeof zero);
+  if (clear && v) {
+    // Clear only the bits just read, atomically on the device: a bit that a
+    // kernel launched meanwhile by another host thread sets stays set.
+    e = lfm::launch_status_clear(v);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(e, "clear status word");
   }
   *status_out = v;

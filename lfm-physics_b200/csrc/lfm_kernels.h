@@ -51,6 +51,8 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream);
 
 // A bounded wait that must give up (failure-detection test, step_tma.cu).
 cudaError_t launch_wait_selftest(int* status, uint64_t limit_ns, cudaStream_t stream);
+// Clears `bits` of the device status word (atomically, on the legacy stream).
+cudaError_t launch_status_clear(int bits);
 
 // S_a pipeline pieces (helmholtz.cu).
 cudaError_t launch_color_energy(const float* pr, const float* pi, float* e, int N,

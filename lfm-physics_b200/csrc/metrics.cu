@@ -205,12 +205,15 @@ cudaError_t launch_metrics(const MetricsArgs& a, double* partials, int rows, dou
 // lfm_metrics_f64 keeps its scratch.
 //
 // The per-CTA partials live in this file-scope device array instead.  Every
-// GPU that loads the library holds it (about 240 KB) until the process ends.
-// One CTA reduces each 65536 cells, so a lattice may have at most
+// GPU that loads the library holds it until the process ends:
+// (kNoAllocRows + 1) rows x kPartialStride (12) doubles = 196,704 bytes
+// (192 KiB).  One CTA reduces each 65536 cells, so a lattice may have at most
 // kNoAllocRows * 65536 cells (N <= 512).  Host code must not pass the
 // array's name to a kernel: on the host it only stands in for the symbol, and
 // the device address comes from cudaGetSymbolAddress, taken once per device
-// on the first call made with that device current.
+// on the first call made with that device current.  That address belongs to
+// the device's primary context (the one the CUDA runtime uses), so calls must
+// be made with the primary context current.
 // ---------------------------------------------------------------------------
 namespace {
 

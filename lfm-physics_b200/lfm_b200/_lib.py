@@ -160,10 +160,32 @@ def tune_get(level: int, N: int) -> dict | None:
 
 
 def device_status(clear: bool = True) -> int:
+    """The device status word (0 = no device-side wait gave up); synchronises the device."""
     v = c_int(0)
     call("lfm_device_status", ctypes.byref(v), 1 if clear else 0)
     return v.value
 
 
+def check_device(where: str, device=None) -> None:
+    """Raise LfmError if a kernel's bounded wait gave up since the last check.
+
+    A step kernel whose wait runs out records LFM_ERR_DEVICE_TIMEOUT in the
+    device status word and returns with its outputs partly written; the host
+    learns of it here (the word is read after a device synchronisation and
+    cleared), so the corrupted state is never returned silently.
+    """
+    if device is not None:
+        import torch
+
+        with torch.cuda.device(device):
+            code = device_status(clear=True)
+    else:
+        code = device_status(clear=True)
+    if code:
+        raise LfmError(code, where, "a device-side wait gave up; the fields written by that "
+                       "launch are incomplete")
+
+
 __all__ = ["MaskLut", "LfmError", "load", "check", "call", "set_step_path", "device_status",
+           "check_device",
            "exported_symbols", "c_float"]

@@ -90,7 +90,9 @@ class B200Backend:
         return self.from_numpy(_host_mask(N, boundary_fraction))
 
     def to_numpy(self, arr) -> np.ndarray:
-        return arr.detach().to("cpu").numpy()
+        out = arr.detach().to("cpu").numpy()
+        _lib.check_device("to_numpy", self.device)
+        return out
 
     def from_numpy(self, arr):
         import torch
@@ -101,6 +103,7 @@ class B200Backend:
         import torch
 
         torch.cuda.synchronize(self.device)
+        _lib.check_device("synchronize", self.device)
 
     # -- argument checks --------------------------------------------------------
     def _ptr(self, t, numel: int, what: str) -> int:

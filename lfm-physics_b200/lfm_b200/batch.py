@@ -251,7 +251,9 @@ class BatchedLattices:
 
     def _host(self, i: int, t) -> np.ndarray:
         N = self._n(i)
-        return t.detach().to("cpu").numpy().reshape(N, N, N)
+        host = t.detach().to("cpu").numpy().reshape(N, N, N)
+        _lib.check_device("BatchedLattices read", self.device)
+        return host
 
     def _imag(self, i: int):
         if self._pi[i] is None:

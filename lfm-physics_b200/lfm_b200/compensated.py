@@ -144,7 +144,9 @@ class CompensatedEvolver:
         return t.reshape(self.N, self.N, self.N)
 
     def _host(self, t) -> np.ndarray:
-        return self._shape(t).detach().to("cpu").numpy()
+        host = self._shape(t).detach().to("cpu").numpy()
+        _lib.check_device("CompensatedEvolver read", self.device)
+        return host
 
     def set_psi_real(self, arr) -> None:
         self._pr[self._cur].copy_(self._dev(arr))

@@ -37,7 +37,17 @@ from .mask import MaskTable
 
 
 class Evolver:
-    """Leapfrog evolver for one lattice on one GPU."""
+    """Leapfrog evolver for one lattice on one GPU.
+
+    ``freeze_chi`` reproduces the reference bit for bit only with
+    ``buffers="ab"``: the reference restores its four chi buffers, two of
+    which are stale in an evolved state, so its frozen chi alternates between
+    two consecutive steps.  The resident layout holds the active (chi,
+    chi_prev) pair instead; the two agree after ``set_chi``.
+
+    Host reads (``get_*``, ``synchronize``) raise ``LfmError`` if a kernel's
+    bounded device-side wait gave up since the last read.
+    """
 
     def __init__(self, config, backend="auto", buffers: str = "resident") -> None:
         import torch
@@ -472,7 +482,17 @@ class Evolver:
         if out is not None:
             out.reshape(-1).copy_(t.reshape(-1), non_blocking=True)
             return out
-        return t.detach().to("cpu").numpy()
+        host = t.detach().to("cpu").numpy()
+        _lib.check_device("Evolver read", self.device)
+        return host
+
+    def synchronize(self) -> None:
+        """Wait for this lattice's queued work; raise LfmError if a kernel's bounded
+        device-side wait gave up (its outputs would be incomplete)."""
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        _lib.check_device("Evolver.synchronize", self.device)
 
     def _current_buf(self) -> str:
         return "A" if self._use_buffer_A else "B"

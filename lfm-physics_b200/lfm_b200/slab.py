@@ -247,6 +247,8 @@ class SlabEvolver:
     def gather(self, field: str) -> np.ndarray:
         """The whole lattice's current field on every rank, (N, N, N) float32."""
         mine = self.local(field).detach().to("cpu").numpy()
+        if self.device.type == "cuda":
+            _lib.check_device("SlabEvolver.gather", self.device)
         if self.world == 1 or self._exchange_fn is not None:
             return mine
         import torch.distributed as dist
@@ -310,6 +312,8 @@ def gather_local(slabs: list, field: str) -> np.ndarray:
     out = np.empty((N, N, N), np.float32)
     for s in slabs:
         out[s.i_first:s.i_first + s.n_local] = s.local(field).detach().to("cpu").numpy()
+        if s.device.type == "cuda":
+            _lib.check_device("gather_local", s.device)
     return out
 
 

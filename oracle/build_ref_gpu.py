@@ -9,9 +9,11 @@ ref_gpu_launch.cu (the launchers) for sm_100a with nvcc's defaults, as NVRTC
 compiles them for CuPy (FMA contraction on, no fast math).  oracle/_ref/ is
 not committed; it travels with the working tree to the GPU machine.
 
-    python oracle/build_ref_gpu.py [REFERENCE_ROOT]
+    python oracle/build_ref_gpu.py REFERENCE_ROOT
 
-Without the reference checkout it does nothing and says so.
+The checkout comes from the argument or, without one, from the
+LFM_REFERENCE_ROOT environment variable.  Without a checkout it does nothing
+and says so.
 """
 
 from __future__ import annotations
@@ -26,7 +28,6 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 LIB = OUT / "libref_gpu.so"
-DEFAULT_REFERENCE = Path("/root/reference")
 NAMES = ("EVOLUTION_REAL_KERNEL_SRC", "EVOLUTION_COMPLEX_KERNEL_SRC", "EVOLUTION_KERNEL_SRC")
 
 
@@ -40,8 +41,13 @@ def _kernel_sources(ref_root: Path) -> str:
 
 
 def build(ref_root: Path | None = None, force: bool = False) -> Path | None:
-    ref_root = Path(ref_root or os.environ.get("LFM_REFERENCE_ROOT", DEFAULT_REFERENCE))
+    ref_root = ref_root or os.environ.get("LFM_REFERENCE_ROOT")
     launcher = HERE / "ref_gpu_launch.cu"
+    if not ref_root:
+        print("no reference checkout given (argument or LFM_REFERENCE_ROOT): "
+              "reference GPU kernels not built")
+        return LIB if LIB.exists() else None
+    ref_root = Path(ref_root)
     if not (ref_root / "lfm" / "core" / "backends" / "kernel_source.py").exists():
         print(f"reference checkout not found at {ref_root}: reference GPU kernels not built")
         return LIB if LIB.exists() else None

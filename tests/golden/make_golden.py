@@ -2,7 +2,7 @@
 
 Run in a checkout that has the reference package importable, e.g.::
 
-    PYTHONPATH=/root/reference PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+    PYTHONPATH=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
 
 Every array here comes from the reference's own code: ``NumpyBackend``
 (lfm/core/backends/numpy_backend.py), ``laplacian_19pt``

@@ -53,3 +53,30 @@ def test_bounded_device_wait_gives_up_and_reports(cuda_device):
     got = np.ascontiguousarray(ev.get_psi_real(), dtype=np.float32).ravel()
     assert np.array_equal(got.view(np.uint32), lat.pr.view(np.uint32))
     assert _lib.device_status() == 0
+
+
+@pytest.mark.gpu
+def test_reads_raise_after_a_device_wait_gave_up(cuda_device):
+    """A timed-out wait is never silent: the next host read of the state raises."""
+    from lfm_b200 import B200Backend, Evolver, _lib
+    from lfm_b200.backend import _stream_handle
+    from lfm_b200.config import gravity_only
+
+    be = B200Backend(cuda_device)
+    N = 16
+    ev = Evolver(gravity_only(N), backend=be)
+    ev.set_psi_real(O.parity_seed_blob(N))
+    ev.evolve(2)
+    ev.get_chi()  # nothing pending: reads normally
+    _lib.call("lfm_selftest_device_timeout", 5_000_000, _stream_handle(be.device))  # 5 ms
+    ev.evolve(1)
+    with pytest.raises(_lib.LfmError) as e:
+        ev.get_psi_real()
+    assert e.value.code & _lib.LFM_ERR_DEVICE_TIMEOUT
+    # the read cleared the word: later reads and synchronize() succeed
+    ev.get_psi_real()
+    ev.synchronize()
+    _lib.call("lfm_selftest_device_timeout", 5_000_000, _stream_handle(be.device))
+    with pytest.raises(_lib.LfmError):
+        be.synchronize()
+    assert _lib.device_status() == 0
