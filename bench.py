@@ -416,27 +416,22 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
     """Gradient of |chi_final - chi_target|^2 through `adjoint_steps` COMPLEX 96^3
     steps (gravity_em: lambda = 4/31, eps_w = 0.1) with respect to the
     amplitude, centre and phase of two packets and a per-cell chi offset; the
-    target is a forward run from perturbed packet parameters (seed 6).
+    target is a forward run from other packet parameters
+    (lfm_b200.workloads.adjoint_packets, seed 6).
     Forward = the checkpointed forward pass, backward = recompute + adjoint."""
-    import math
-
     import torch
 
     from lfm_b200 import Evolver
     from lfm_b200.adjoint import leapfrog, memory_bytes, soliton_state
     from lfm_b200.config import gravity_em
+    from lfm_b200.workloads import adjoint_packets
 
-    N, steps, sigma = 96, args.adjoint_steps, 3.0
+    N, steps = 96, args.adjoint_steps
     cfg = gravity_em(N)
-    g = torch.Generator().manual_seed(6)
-    amp = 2.0 + 2.0 * torch.rand(2, generator=g)
-    cen = torch.tensor([[N / 2 - 10.0, N / 2, N / 2], [N / 2 + 10.0, N / 2, N / 2]])
-    ph = 2.0 * math.pi * torch.rand(2, generator=g)
-    pert = (amp * (1.0 + 0.05 * torch.randn(2, generator=g)),
-            cen + 0.5 * torch.randn(2, 3, generator=g), ph + 0.1 * torch.randn(2, generator=g))
-    params = [t.to(dev) for t in (amp, cen, ph)]
+    (amp, cen, ph), pert, sigma = adjoint_packets(N)
+    params = [t.to(dev).float() for t in (amp, cen, ph)]
     with torch.no_grad():
-        st = soliton_state(N, *[t.to(dev) for t in pert], sigma, cfg.chi0, None, True)
+        st = soliton_state(N, *[t.to(dev).float() for t in pert], sigma, cfg.chi0, None, True)
         target = leapfrog(cfg, st, steps, backend=be)[4].clone()
     stream = torch.cuda.current_stream(dev)
 

@@ -123,3 +123,32 @@ def sweep_lattices(count: int = 256, seed: int = 5, sizes=(32, 48, 64, 80, 96)):
             pi = pi.astype(np.float32)
         out.append((cfg, pr.astype(np.float32), pi))
     return out
+
+
+def adjoint_packets(N: int = 96, seed: int = 6):
+    """Adjoint workload: the learnable packets and the target run's packets.
+
+    Two packets of sigma 3 cells, 8 cells apart along j around the centre (they
+    overlap, so their relative phase shapes |Psi|^2 and the momentum current),
+    amplitudes U[4, 6] and phases U[0, 2 pi) (seed).  The target run uses
+    different parameters drawn from the same generator: amplitudes x U[1.15,
+    1.35], centres moved by U[-2, 2] cells per axis, phases moved by U[-0.8,
+    0.8].  chi's deviation from chi0 then differs between the two runs by a
+    sizeable fraction of itself, so the loss |chi_T - chi_target|^2 and its
+    gradients stand well above float32 rounding.
+
+    Returns ((amplitude (2,), centre (2, 3), phase (2,)), (the target's three),
+    sigma), float64 torch tensors on the CPU.
+    """
+    import torch
+
+    g = torch.Generator().manual_seed(seed)
+    u = lambda *s: torch.rand(*s, generator=g, dtype=torch.float64)  # noqa: E731
+    c = N / 2.0
+    amp = 4.0 + 2.0 * u(2)
+    cen = torch.tensor([[c, c - 4.0, c], [c, c + 4.0, c]], dtype=torch.float64)
+    ph = 2.0 * math.pi * u(2)
+    amp_t = amp * (1.15 + 0.2 * u(2))
+    cen_t = cen + (4.0 * u(2, 3) - 2.0)
+    ph_t = ph + (1.6 * u(2) - 0.8)
+    return (amp, cen, ph), (amp_t, cen_t, ph_t), 3.0
