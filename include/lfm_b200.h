@@ -189,6 +189,35 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
                                   double e0_sq, double epsilon_w, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Split-chi steps.  No counterpart kernel in the reference; they advance the
+ * equations of lfm_leapfrog_real_f32 / _complex_f32 (numpy_backend.py:80-205)
+ * close to float64 accuracy.
+ *
+ * chi is held as chi0 + hi + lo, two float32 slots per time level (hi, and lo
+ * the part below one ulp of hi); Psi as in the plain resident step.  The chi
+ * update and every acceleration term involving chi run in float64, the
+ * Laplacians in float32 (hi's from neighbour differences).  The slots rotate
+ * as in lfm_leapfrog_real_f32: each call reads (cur, prev) of every field and
+ * writes the new values over prev; damp_prev as there (Psi's previous slot is
+ * multiplied by (1 - mask) on read).  chi's previous slots are undamped.
+ * Moves 36 B/cell (REAL), 48 B (COMPLEX).  Lattices with N % 4 != 0 take the
+ * direct kernel, with the same results.
+ * ------------------------------------------------------------------------ */
+int lfm_leapfrog_real_split_f32(const float* psi, float* psi_prev_io, const float* chi_hi,
+                                float* chi_hi_prev_io, const float* chi_lo, float* chi_lo_prev_io,
+                                const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                                int N, double dt2, double kappa, double lambda_self, double chi0,
+                                double e0_sq, void* stream);
+
+int lfm_leapfrog_complex_split_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                                   float* psi_i_prev_io, const float* chi_hi,
+                                   float* chi_hi_prev_io, const float* chi_lo,
+                                   float* chi_lo_prev_io, const float* mask_table,
+                                   const lfm_mask_lut* lut, int damp_prev, int N, double dt2,
+                                   double kappa, double lambda_self, double chi0, double e0_sq,
+                                   double epsilon_w, void* stream);
+
+/* ------------------------------------------------------------------------
  * Poisson equilibration of chi (lfm/fields/equilibrium.py:26-121, as
  * Simulation.equilibrate calls it, lfm/simulation.py:877-963):
  * chi = chi0 + dchi with  laplacian(dchi) = kappa (|Psi|^2 - e0_sq)  solved

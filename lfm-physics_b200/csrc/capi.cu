@@ -810,6 +810,67 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
+int lfm_leapfrog_real_split_f32(const float* psi, float* psi_prev_io, const float* chi_hi,
+                                float* chi_hi_prev_io, const float* chi_lo, float* chi_lo_prev_io,
+                                const float* mask_table, const lfm_mask_lut* lut, int damp_prev,
+                                int N, double dt2, double kappa, double lambda_self, double chi0,
+                                double e0_sq, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi || !psi_prev_io || !chi_hi || !chi_hi_prev_io || !chi_lo || !chi_lo_prev_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi, b}, {chi_hi, b}, {chi_lo, b}},
+                      {{psi_prev_io, b}, {chi_hi_prev_io, b}, {chi_lo_prev_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_REAL;
+  a.N = N;
+  a.split = 1;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, 0, 0, 0, 0, 0);
+  a.pr = psi; a.pr_prev = psi_prev_io; a.pr_out = psi_prev_io;
+  a.chi = chi_hi; a.chi_prev = chi_hi_prev_io; a.chi_out = chi_hi_prev_io;
+  a.chi_lo = chi_lo; a.chi_lo_prev = chi_lo_prev_io; a.chi_lo_out = chi_lo_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
+int lfm_leapfrog_complex_split_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                                   float* psi_i_prev_io, const float* chi_hi,
+                                   float* chi_hi_prev_io, const float* chi_lo,
+                                   float* chi_lo_prev_io, const float* mask_table,
+                                   const lfm_mask_lut* lut, int damp_prev, int N, double dt2,
+                                   double kappa, double lambda_self, double chi0, double e0_sq,
+                                   double epsilon_w, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!psi_r || !psi_r_prev_io || !psi_i || !psi_i_prev_io || !chi_hi || !chi_hi_prev_io ||
+      !chi_lo || !chi_lo_prev_io)
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{psi_r, b}, {psi_i, b}, {chi_hi, b}, {chi_lo, b}},
+                      {{psi_r_prev_io, b}, {psi_i_prev_io, b}, {chi_hi_prev_io, b},
+                       {chi_lo_prev_io, b}});
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = LFM_COMPLEX;
+  a.N = N;
+  a.split = 1;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, epsilon_w, 0, 0, 0, 0);
+  a.pr = psi_r; a.pr_prev = psi_r_prev_io; a.pr_out = psi_r_prev_io;
+  a.pi = psi_i; a.pi_prev = psi_i_prev_io; a.pi_out = psi_i_prev_io;
+  a.chi = chi_hi; a.chi_prev = chi_hi_prev_io; a.chi_out = chi_hi_prev_io;
+  a.chi_lo = chi_lo; a.chi_lo_prev = chi_lo_prev_io; a.chi_lo_out = chi_lo_prev_io;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
 int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
                          float* sa_raw, int N, double sa_gamma, double sa_d, void* stream) {
   int rc = check_n(N);

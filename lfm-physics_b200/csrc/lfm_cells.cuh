@@ -415,3 +415,123 @@ __device__ __forceinline__ ComplexComp complex_cell_comp(float lapR, float pr, f
 }
 
 }  // namespace lfm
+
+// ---- split chi (two-float offset from chi0) -----------------------------------
+//
+// chi is held as chi0 + hi + lo with hi, lo float32 and lo the part of the
+// offset below one ulp of hi (about 48 significant bits in all).  Psi stays
+// one float32 per value.  Float32 storage of chi itself is what limits the
+// plain path's accuracy against float64: chi ~ 19 keeps only ~2e-6 of
+// absolute precision, its per-step increments are rounded away, and Psi's
+// frequency follows chi.  Here the chi update and every acceleration term that
+// involves chi run in float64; the Laplacians stay float32: hi's by
+// neighbour-minus-centre differences (exact for nearby values), lo's directly
+// (its values are below one ulp of hi).  The update is the reference's
+// (numpy_backend.py:80-205) in exact arithmetic:
+//   Psi' = (1-m)(2 Psi - Psi_prev + dt2 (lap Psi - chi^2 Psi))
+//   d'   = (1-m) max(2 d - d_prev + dt2 acc_chi, -2 chi0),   d = chi - chi0
+// (the sponge blend m chi0 + (1-m) chi_new and the clamp chi >= -chi0 in
+// offset form).  Every operation is an explicit _rn intrinsic, so the fused
+// and the direct kernels give the same bits.
+namespace lfm {
+
+__device__ __forceinline__ double split_value(float hi, float lo) {
+  return __dadd_rn((double)hi, (double)lo);
+}
+
+// lap(chi) = lap(hi) + lap(lo), in float32.
+__device__ __forceinline__ float lap_split(const S19& H, const S19& L) {
+  return __fadd_rn(lap19_diff(H), lap19_fma(L));
+}
+
+// One Psi component: the acceleration lap - chi^2 p in float64, rounded once,
+// then p_new = dt2 * acc + (2p - p_prev) in float32 (not yet absorbed).
+__device__ __forceinline__ float split_psi(float lap, float p, float p_prev, double chi_sq,
+                                           const StepConsts& s) {
+  const float acc = __double2float_rn(__fma_rn(-chi_sq, (double)p, (double)lap));
+  return __fmaf_rn(s.dt2, acc, __fmaf_rn(2.0f, p, -p_prev));
+}
+
+struct SplitChi {
+  float hi, lo;
+};
+
+// chi offset update in float64 from its acceleration; split back into two floats.
+__device__ __forceinline__ SplitChi split_chi(double d, double d_prev, double acc, float mask,
+                                              const StepConsts& s) {
+  double dn = __fma_rn(s.dt2_d, acc, __dsub_rn(__dadd_rn(d, d), d_prev));
+  const double lim = -2.0 * s.chi0_d;
+  dn = dn < lim ? lim : dn;  // chi >= -chi0; a NaN stays NaN
+  dn = __dmul_rn(__dsub_rn(1.0, (double)mask), dn);
+  SplitChi o;
+  o.hi = __double2float_rn(dn);
+  o.lo = __double2float_rn(__dsub_rn(dn, (double)o.hi));
+  return o;
+}
+
+// Mexican-hat term of the chi acceleration, float64.
+__device__ __forceinline__ double split_hat(double acc, double chi, double chi_sq,
+                                            const StepConsts& s) {
+  if (!s.use_lambda) return acc;
+  return __fma_rn(-__dmul_rn(s.four_lambda_d, chi), __dsub_rn(chi_sq, s.chi0_sq_d), acc);
+}
+
+struct RealSplit {
+  float psi;  // new E, absorbed (stored)
+  SplitChi chi;
+};
+
+// REAL: lapE = lap19_fma(E), lapD = lap_split(H, L); e_prev as the reference
+// reads it (absorbed); d, d_prev the chi offsets (split_value).
+__device__ __forceinline__ RealSplit real_cell_split(float lapE, float e, float e_prev, float lapD,
+                                                     double d, double d_prev, float mask,
+                                                     float absorb, const StepConsts& s) {
+  const double chi = __dadd_rn(s.chi0_d, d);
+  const double chi_sq = __dmul_rn(chi, chi);
+  const float e_new = split_psi(lapE, e, e_prev, chi_sq, s);
+  const double ed = (double)e;
+  const double src =
+      __dmul_rn(__dmul_rn(s.k_over_chi0_d, chi), __fma_rn(ed, ed, -s.e0_sq_d));
+  const double acc = split_hat(__dsub_rn((double)lapD, src), chi, chi_sq, s);
+  RealSplit o;
+  o.psi = __fmul_rn(e_new, absorb);
+  o.chi = split_chi(d, d_prev, acc, mask, s);
+  return o;
+}
+
+struct ComplexSplit {
+  float pr, pi;  // absorbed (stored)
+  SplitChi chi;
+};
+
+// COMPLEX: the momentum current from float32 neighbour differences (exact for
+// nearby values), its products and sums in float64.
+__device__ __forceinline__ ComplexSplit complex_cell_split(float lapR, float pr, float pr_prev,
+                                                           const Faces& R, float lapI, float pi,
+                                                           float pi_prev, const Faces& I,
+                                                           float lapD, double d, double d_prev,
+                                                           float mask, float absorb,
+                                                           const StepConsts& s) {
+  const double chi = __dadd_rn(s.chi0_d, d);
+  const double chi_sq = __dmul_rn(chi, chi);
+  const float r_new = split_psi(lapR, pr, pr_prev, chi_sq, s);
+  const float i_new = split_psi(lapI, pi, pi_prev, chi_sq, s);
+  const double prd = (double)pr, pid = (double)pi;
+  const double psi_sq = __fma_rn(prd, prd, __dmul_rn(pid, pid));
+  auto axis = [&](float rp, float rm, float ip, float im) {
+    return __fma_rn(prd, (double)__fsub_rn(ip, im), -__dmul_rn(pid, (double)__fsub_rn(rp, rm)));
+  };
+  const double jt = __dmul_rn(0.5, __dadd_rn(__dadd_rn(axis(R.ip, R.im, I.ip, I.im),
+                                                       axis(R.jp, R.jm, I.jp, I.jm)),
+                                             axis(R.kp, R.km, I.kp, I.km)));
+  const double q = __dsub_rn(__fma_rn(s.eps_w_d, jt, psi_sq), s.e0_sq_d);
+  const double src = __dmul_rn(__dmul_rn(s.k_over_chi0_d, chi), q);
+  const double acc = split_hat(__dsub_rn((double)lapD, src), chi, chi_sq, s);
+  ComplexSplit o;
+  o.pr = __fmul_rn(r_new, absorb);
+  o.pi = __fmul_rn(i_new, absorb);
+  o.chi = split_chi(d, d_prev, acc, mask, s);
+  return o;
+}
+
+}  // namespace lfm

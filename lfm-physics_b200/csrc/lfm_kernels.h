@@ -34,6 +34,12 @@ struct StepArgs {
   float* sa_clip_out;  // clipped S_a copy (protocol colour step) or null
   int damp_prev;       // multiply the previous-step fields by (1-mask) on read
   int comp;            // compensated Delta form: *_prev hold increments, updated in place
+  // Split chi (REAL, COMPLEX; resident layout only): chi = chi0 + hi + lo with
+  // hi in chi / chi_prev / chi_out and lo in the three pointers below.
+  int split;
+  const float* chi_lo;
+  const float* chi_lo_prev;
+  float* chi_lo_out;
   int* status;         // device status word for bounded waits
   // Slab of a lattice split along i (slab == 0: the whole periodic lattice).
   // The arrays hold ni planes of N x N; the step updates planes [i_lo, i_hi)

@@ -115,6 +115,9 @@ struct StepConsts {
   int use_cc;          // epsilon_cc > 0    (numpy_backend.py:254)
   int use_fc;          // kappa_c > 0       (numpy_backend.py:314)
   int use_ccv;         // kappa_string > 0  (numpy_backend.py:249)
+  // The same parameters unrounded, for the split-chi steps, which evaluate
+  // the accelerations in float64 (lfm_cells.cuh, "split chi").
+  double dt2_d, k_over_chi0_d, four_lambda_d, chi0_d, chi0_sq_d, e0_sq_d, eps_w_d;
 };
 
 inline StepConsts make_step_consts(double dt2, double kappa, double lambda_self, double chi0,
@@ -137,6 +140,13 @@ inline StepConsts make_step_consts(double dt2, double kappa, double lambda_self,
   c.use_cc = eps_cc > 0.0;
   c.use_fc = kappa_c > 0.0;
   c.use_ccv = kappa_string > 0.0;
+  c.dt2_d = dt2;
+  c.k_over_chi0_d = kappa / chi0;
+  c.four_lambda_d = 4.0 * lambda_self;
+  c.chi0_d = chi0;
+  c.chi0_sq_d = chi0 * chi0;
+  c.e0_sq_d = e0_sq;
+  c.eps_w_d = eps_w;
   return c;
 }
 

@@ -49,6 +49,34 @@ __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
     const float absorb = fsub(1.0f, mask);
     const S19 X = gather(a.chi, ix);
     const float chi_prev = a.chi_prev[x];
+    if (LEVEL != LFM_COLOR && a.split) {
+      // split chi: chi = chi0 + hi + lo (resident slots, previous Psi damped on read)
+      const S19 L = gather(a.chi_lo, ix);
+      const float lapD = lap_split(X, L);
+      const double d = split_value(X.c, L.c);
+      const double d_prev = split_value(chi_prev, a.chi_lo_prev[x]);
+      SplitChi c;
+      if (LEVEL == LFM_REAL) {
+        const S19 E = gather(a.pr, ix);
+        const RealSplit o = real_cell_split(lap19_fma(E), E.c, prev_value(a, a.pr_prev, x, absorb),
+                                            lapD, d, d_prev, mask, absorb, a.c);
+        a.pr_out[x] = o.psi;
+        c = o.chi;
+      } else {
+        const S19 R = gather(a.pr, ix);
+        const S19 I = gather(a.pi, ix);
+        const ComplexSplit o = complex_cell_split(
+            lap19_fma(R), R.c, prev_value(a, a.pr_prev, x, absorb), faces_of(R), lap19_fma(I),
+            I.c, prev_value(a, a.pi_prev, x, absorb), faces_of(I), lapD, d, d_prev, mask, absorb,
+            a.c);
+        a.pr_out[x] = o.pr;
+        a.pi_out[x] = o.pi;
+        c = o.chi;
+      }
+      a.chi_out[x] = c.hi;
+      a.chi_lo_out[x] = c.lo;
+      continue;
+    }
     if (LEVEL != LFM_COLOR && a.comp) {
       // compensated Delta form: *_prev hold the increments (updated in place)
       if (LEVEL == LFM_REAL) {

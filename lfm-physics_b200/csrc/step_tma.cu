@@ -38,6 +38,9 @@ namespace lfm {
 namespace {
 
 constexpr int kMaxStencil = 7;
+// Step forms of the register-queue kernel: the reference's float32 step
+// (bit-exact), the compensated Delta form, and split chi (chi0 + hi + lo).
+constexpr int kPlain = 0, kComp = 1, kSplit = 2;
 constexpr int kMaxPoint = 11;
 constexpr int kMaxStages = 6;
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per wait
@@ -525,8 +528,8 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
 }
 
 // The register-queue kernels that copy a stencil field's rows as one (above).
-template <int LEVEL, bool COMP>
-constexpr bool kOneCopy = LEVEL == LFM_COMPLEX || COMP;
+template <int LEVEL, int MODE>
+constexpr bool kOneCopy = LEVEL == LFM_COMPLEX || MODE != kPlain;
 
 template <int LEVEL, int V>
 __global__ void __launch_bounds__(512) tma_step_kernel(const __grid_constant__ TmaParams P) {
@@ -735,9 +738,10 @@ __device__ __forceinline__ Faces faces_of(const S19& s) {
   return f;
 }
 
-template <int LEVEL>
+// Stencil fields of the march: Psi components and chi (split chi: hi, lo).
+template <int LEVEL, int MODE = kPlain>
 struct QFields {
-  static constexpr int ns = (LEVEL == LFM_REAL) ? 2 : 3;
+  static constexpr int ns = ((LEVEL == LFM_REAL) ? 2 : 3) + (MODE == kSplit ? 1 : 0);
 };
 
 // Tile geometry of a march.  GeomRT reads it from the parameters (any
@@ -785,17 +789,17 @@ struct QShared {
 // CTA must stop (a bounded wait gave up).
 // SCUR / SNXT: the stages of the centre and the next plane when the
 // geometry fixes them (3 stages, the loop unrolled by 3), else -1.
-template <int LEVEL, int V, bool COMP, bool PARTIAL, int PA, int PB, int PC, class G = GeomRT,
+template <int LEVEL, int V, int MODE, bool PARTIAL, int PA, int PB, int PC, class G = GeomRT,
           int SCUR = -1, int SNXT = -1>
 __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_t* bars,
-                                        QShared& sh, QPlane<V> (&Q)[QFields<LEVEL>::ns][3],
+                                        QShared& sh, QPlane<V> (&Q)[QFields<LEVEL, MODE>::ns][3],
                                         const QLane& L, int c, int i0, int i1, int j0,
                                         int nplanes, int nwarps, int& s_cur_rt, int& s_nxt_rt,
                                         uint32_t& ph_nxt, const QKeys<V>& K,
                                         bool lane_active) {
   // PARTIAL: the CTA may be wider than the tile (batch kernel)
   const bool active = !PARTIAL || lane_active;
-  constexpr int NS = QFields<LEVEL>::ns;
+  constexpr int NS = QFields<LEVEL, MODE>::ns;
   const StepArgs& a = P.a;
   const G g(P);
   const int N = g.N, TJ = g.TJ;
@@ -843,7 +847,54 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
 #pragma unroll
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
   const int64_t gofs = ((int64_t)i * N + j) * N + k0;
-  if constexpr (COMP) {
+  if constexpr (MODE == kSplit) {
+    // Split chi: stencil fields Psi (Psi_r, Psi_i), hi, lo; point fields their
+    // previous slots in the same order.  New values go over the previous slots.
+    if constexpr (LEVEL == LFM_REAL) {
+      const Vec<V> ep = lds<V>(smem, bc + L.o_pt);
+      const Vec<V> hp = lds<V>(smem, bc + L.o_pt + PTS);
+      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+      float o_e[V], o_h[V], o_l[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const S19 E = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 H = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const S19 Lo = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
+        const float epv = a.damp_prev ? fmul(ep.v[e], absorb[e]) : ep.v[e];
+        const RealSplit o =
+            real_cell_split(lap19_fma(E), E.c, epv, lap_split(H, Lo), split_value(H.c, Lo.c),
+                            split_value(hp.v[e], lp.v[e]), mask[e], absorb[e], a.c);
+        o_e[e] = o.psi; o_h[e] = o.chi.hi; o_l[e] = o.chi.lo;
+      }
+      stg<V>(a.pr_out + gofs, o_e);
+      stg<V>(a.chi_out + gofs, o_h);
+      stg<V>(a.chi_lo_out + gofs, o_l);
+    } else {
+      const Vec<V> rp = lds<V>(smem, bc + L.o_pt);
+      const Vec<V> ip = lds<V>(smem, bc + L.o_pt + PTS);
+      const Vec<V> hp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 3 * PTS);
+      float o_r[V], o_i[V], o_h[V], o_l[V];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const S19 R = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
+        const S19 I = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
+        const S19 H = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
+        const S19 Lo = q_s19<V>(Q[3][PA], Q[3][PB], Q[3][PC], e);
+        const float rpv = a.damp_prev ? fmul(rp.v[e], absorb[e]) : rp.v[e];
+        const float ipv = a.damp_prev ? fmul(ip.v[e], absorb[e]) : ip.v[e];
+        const ComplexSplit o = complex_cell_split(
+            lap19_fma(R), R.c, rpv, faces_of(R), lap19_fma(I), I.c, ipv, faces_of(I),
+            lap_split(H, Lo), split_value(H.c, Lo.c), split_value(hp.v[e], lp.v[e]), mask[e],
+            absorb[e], a.c);
+        o_r[e] = o.pr; o_i[e] = o.pi; o_h[e] = o.chi.hi; o_l[e] = o.chi.lo;
+      }
+      stg<V>(a.pr_out + gofs, o_r);
+      stg<V>(a.pi_out + gofs, o_i);
+      stg<V>(a.chi_out + gofs, o_h);
+      stg<V>(a.chi_lo_out + gofs, o_l);
+    }
+  } else if constexpr (MODE == kComp) {
     // Delta form: point fields hold the increments; new values go to the
     // *_out buffers, new increments over the increments (*_prev_out).
     if constexpr (LEVEL == LFM_REAL) {
@@ -986,7 +1037,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       sh.done[s_cur] = 0u;
       fence_proxy_async_smem();
       if (c + 1 + g.S < nplanes) {
-        issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, c + 1 + g.S, i0, i1, j0);
+        issue_plane<G::kSlab, true, kOneCopy<LEVEL, MODE>>(P, smem, bars, c + 1 + g.S, i0, i1, j0);
         atomicMax(&sh.issued, c + 2 + g.S);
       }
     }
@@ -1005,10 +1056,10 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
 // The march of one tile: rows j0 .. j0+rows-1 (all k), planes [i0, i1).
 // Initialises the stage barriers and the bookkeeping itself, so a CTA may
 // run several marches one after another (the batch kernel).
-template <int LEVEL, int V, bool COMP, bool PARTIAL, class G = GeomRT>
+template <int LEVEL, int V, int MODE, bool PARTIAL, class G = GeomRT>
 __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_t* bars,
                                         QShared& sh, int j0, int i0, int i1, int rows) {
-  constexpr int NS = QFields<LEVEL>::ns;
+  constexpr int NS = QFields<LEVEL, MODE>::ns;
   const G g(P);
   const int N = g.N, TJ = g.TJ, S = g.S;
   const int n = i1 - i0;
@@ -1066,7 +1117,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     }
     const int first = min(S, nplanes);
     for (int u = 0; u < first; ++u)
-      issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, u, i0, i1, j0);
+      issue_plane<G::kSlab, true, kOneCopy<LEVEL, MODE>>(P, smem, bars, u, i0, i1, j0);
     sh.issued = first;
   }
   if (tab_at >= 0) {
@@ -1097,7 +1148,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     // stage 0 (plane i0-1) is dead: refill it with u = S
     if (tid == 0 && S < nplanes) {
       fence_proxy_async_smem();
-      issue_plane<G::kSlab, true, kOneCopy<LEVEL, COMP>>(P, smem, bars, S, i0, i1, j0);
+      issue_plane<G::kSlab, true, kOneCopy<LEVEL, MODE>>(P, smem, bars, S, i0, i1, j0);
       sh.issued = S + 1;
     }
     int s_cur = 1 % S, s_nxt = 2 % S;
@@ -1107,15 +1158,15 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
     // has its centre plane in stage (p + 1) % 3 and the next in (p + 2) % 3.
     constexpr bool F = G::kStages == 3;
     while (true) {
-      if (c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 0, 1, 2, G, F ? 1 : -1, F ? 2 : -1>(
+      if (c >= n || !q_plane<LEVEL, V, MODE, PARTIAL, 0, 1, 2, G, F ? 1 : -1, F ? 2 : -1>(
                         P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
                         ph_nxt, K, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 1, 2, 0, G, F ? 2 : -1, F ? 0 : -1>(
+      if (++c >= n || !q_plane<LEVEL, V, MODE, PARTIAL, 1, 2, 0, G, F ? 2 : -1, F ? 0 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
                           ph_nxt, K, active))
         break;
-      if (++c >= n || !q_plane<LEVEL, V, COMP, PARTIAL, 2, 0, 1, G, F ? 0 : -1, F ? 1 : -1>(
+      if (++c >= n || !q_plane<LEVEL, V, MODE, PARTIAL, 2, 0, 1, G, F ? 0 : -1, F ? 1 : -1>(
                           P, smem, bars, sh, Q, L, c, i0, i1, j0, nplanes, nwarps, s_cur, s_nxt,
                           ph_nxt, K, active))
         break;
@@ -1131,7 +1182,7 @@ __device__ __forceinline__ void q_march(const TmaParams& P, float* smem, uint64_
   }
 }
 
-template <int LEVEL, int V, bool COMP, class G = GeomRT>
+template <int LEVEL, int V, int MODE, class G = GeomRT>
 __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ TmaParams P) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
@@ -1141,7 +1192,7 @@ __global__ void __launch_bounds__(512) tma_queue_kernel(const __grid_constant__ 
   const bool slab = G::kSlab && P.a.slab;
   const int lo = slab ? P.a.i_lo : 0, hi = slab ? P.a.i_hi : g.N;
   const int i0 = lo + ch * P.IC;
-  q_march<LEVEL, V, COMP, false, G>(P, smem, bars, sh, jt * g.TJ, i0, min(i0 + P.IC, hi), g.TJ);
+  q_march<LEVEL, V, MODE, false, G>(P, smem, bars, sh, jt * g.TJ, i0, min(i0 + P.IC, hi), g.TJ);
 }
 
 // ---- batch kernel: many lattices, one launch per step -------------------------
@@ -1218,7 +1269,7 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
       batch_params<LEVEL>(P, L, B, it.j1 - it.j0);
     }
     __syncthreads();  // P is visible to every thread
-    q_march<LEVEL, V, false, true, GeomRTT<TABM>>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
+    q_march<LEVEL, V, kPlain, true, GeomRTT<TABM>>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
     __syncthreads();  // every wait of the march is over
     if (sh.abort_flag) break;  // same value in every thread
     if (threadIdx.x == 0)
@@ -1389,36 +1440,36 @@ cudaError_t launch_kernel(K kernel, int* granted, std::mutex* mu, const TmaParam
   return cudaGetLastError();
 }
 
-template <int LEVEL, int V, bool QUEUE, bool COMP>
+template <int LEVEL, int V, bool QUEUE, int MODE>
 struct KernelSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
     if constexpr (QUEUE)
-      return tma_queue_kernel<LEVEL, V, COMP>;
+      return tma_queue_kernel<LEVEL, V, MODE>;
     else
       return tma_step_kernel<LEVEL, V>;
   }
 };
-template <int LEVEL, int V, bool QUEUE, bool COMP>
-std::mutex KernelSlot<LEVEL, V, QUEUE, COMP>::mu;
-template <int LEVEL, int V, bool QUEUE, bool COMP>
-int KernelSlot<LEVEL, V, QUEUE, COMP>::granted = 0;
+template <int LEVEL, int V, bool QUEUE, int MODE>
+std::mutex KernelSlot<LEVEL, V, QUEUE, MODE>::mu;
+template <int LEVEL, int V, bool QUEUE, int MODE>
+int KernelSlot<LEVEL, V, QUEUE, MODE>::granted = 0;
 
-// Compile-time tiles for the headline sizes (resident layout); COMP: the
-// compensated (Delta-form) step on the same tile.
-template <int LEVEL, int V, int N, int TJ, int S, bool COMP = false>
+// Compile-time tiles for the headline sizes (resident layout); MODE kComp:
+// the compensated (Delta-form) step on the same tile.
+template <int LEVEL, int V, int N, int TJ, int S, int MODE = kPlain>
 struct FixedSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
-    return tma_queue_kernel<LEVEL, V, COMP, GeomCT<N, TJ, QFields<LEVEL>::ns, S>>;
+    return tma_queue_kernel<LEVEL, V, MODE, GeomCT<N, TJ, QFields<LEVEL, MODE>::ns, S>>;
   }
 };
-template <int LEVEL, int V, int N, int TJ, int S, bool COMP>
-std::mutex FixedSlot<LEVEL, V, N, TJ, S, COMP>::mu;
-template <int LEVEL, int V, int N, int TJ, int S, bool COMP>
-int FixedSlot<LEVEL, V, N, TJ, S, COMP>::granted = 0;
+template <int LEVEL, int V, int N, int TJ, int S, int MODE>
+std::mutex FixedSlot<LEVEL, V, N, TJ, S, MODE>::mu;
+template <int LEVEL, int V, int N, int TJ, int S, int MODE>
+int FixedSlot<LEVEL, V, N, TJ, S, MODE>::granted = 0;
 
 struct FixedTile {
   int level, V, N, TJ, S;
@@ -1441,14 +1492,17 @@ const FixedTile* fixed_tile(int level, int V, int N) {
   return nullptr;
 }
 
-template <int LEVEL, int V, int N, int TJ, bool COMP = false>
+template <int LEVEL, int V, int N, int TJ, int MODE = kPlain>
 cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ), COMP>;
+  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ), MODE>;
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
 
-// The compensated step has a compile-time tile at the throughput size only.
-constexpr bool comp_fixed(int level, int N) { return level == LFM_REAL && N == 512; }
+// Which step forms have compile-time tiles: the plain step at every size of
+// kFixedTiles, the compensated step at the throughput size only, split chi none.
+constexpr bool has_fixed(int mode, int level, int N) {
+  return mode == kPlain || (mode == kComp && level == LFM_REAL && N == 512);
+}
 
 // Shared memory of the sponge table of the compile-time tiles: count entries
 // between a 0 and a 1, after 3 floats of padding that put the first entry on a
@@ -1458,17 +1512,19 @@ int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
 // Launches the compile-time variant when the chosen tile is one of
 // kFixedTiles (no streamed mask or S_a) and its ring plus the sponge table fit
 // in shared memory (ch.smem includes the table then); false if not.
-template <int LEVEL, int V, bool COMP = false>
+template <int LEVEL, int V, int MODE = kPlain>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
   if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
-  if (COMP && !comp_fixed(LEVEL, P.N)) return false;
+  if (!has_fixed(MODE, LEVEL, P.N)) return false;
   const FixedTile* t = fixed_tile(LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
   if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
     return false;
-  if constexpr (COMP) {
+  if constexpr (MODE == kSplit) {
+    return false;
+  } else if constexpr (MODE == kComp) {
     if constexpr (LEVEL == LFM_REAL && V == 4) {
-      *err = launch_fixed<LEVEL, V, 512, 4, true>(P, ch, stream);
+      *err = launch_fixed<LEVEL, V, 512, 4, kComp>(P, ch, stream);
       return true;
     }
     return false;
@@ -1484,9 +1540,9 @@ bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t*
   return false;
 }
 
-template <int LEVEL, int V, bool QUEUE, bool COMP = false>
+template <int LEVEL, int V, bool QUEUE, int MODE = kPlain>
 cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t stream) {
-  using Slot = KernelSlot<LEVEL, V, QUEUE, COMP>;
+  using Slot = KernelSlot<LEVEL, V, QUEUE, MODE>;
   int regs = 0;
   cudaError_t e = kernel_regs(Slot::fn(), &regs);
   if (e != cudaSuccess) return e;
@@ -1503,7 +1559,7 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
   // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
-  const FixedTile* ft = (QUEUE && (!COMP || comp_fixed(LEVEL, P.N)) && P.pf_mask < 0 &&
+  const FixedTile* ft = (QUEUE && has_fixed(MODE, LEVEL, P.N) && P.pf_mask < 0 &&
                          P.pf_sa < 0 && P.np == P.ns && !P.a.slab)
                             ? fixed_tile(LEVEL, V, P.N) : nullptr;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
@@ -1533,7 +1589,7 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   tune_record(LEVEL, P.N, used);
   if constexpr (QUEUE) {
     cudaError_t fe = cudaSuccess;
-    if (try_fixed<LEVEL, V, COMP>(P, ch, stream, &fe)) return fe;
+    if (try_fixed<LEVEL, V, MODE>(P, ch, stream, &fe)) return fe;
   }
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
@@ -1574,7 +1630,18 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   P.tab_off = -1;  // set by the planner when the table goes to shared memory
   P.pf_sa = -1;
   const int64_t n3 = (int64_t)N * N * N;
-  if (a.level == LFM_REAL) {
+  if (a.split) {
+    // split chi: stencil fields Psi..., hi, lo; point fields their previous slots
+    if (a.level == LFM_COLOR || a.comp || a.mask || !a.chi_lo || !a.chi_lo_prev ||
+        !a.chi_lo_out)
+      return cudaErrorNotSupported;
+    int f = 0;
+    P.sf[f] = a.pr; P.pf[f++] = a.pr_prev;
+    if (a.level == LFM_COMPLEX) { P.sf[f] = a.pi; P.pf[f++] = a.pi_prev; }
+    P.sf[f] = a.chi; P.pf[f++] = a.chi_prev;
+    P.sf[f] = a.chi_lo; P.pf[f++] = a.chi_lo_prev;
+    P.ns = P.np = f;
+  } else if (a.level == LFM_REAL) {
     P.ns = 2;
     P.sf[0] = a.pr; P.sf[1] = a.chi;
     P.pf[0] = a.pr_prev; P.pf[1] = a.chi_prev;
@@ -1607,21 +1674,28 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   // every copy source and every vector store needs 16-byte alignment
   const void* ptrs[] = {a.pr, a.pi, a.chi, a.pr_prev, a.pi_prev, a.chi_prev, a.pr_out, a.pi_out,
                         a.chi_out, a.pr_prev_out, a.pi_prev_out, a.chi_prev_out, a.mask, a.sa,
-                        a.sa_clip_out};
+                        a.sa_clip_out, a.chi_lo, a.chi_lo_prev, a.chi_lo_out};
   for (const void* p : ptrs)
     if (p && !aligned16(p)) return cudaErrorNotSupported;
 
   TileConfig forced_cfg;
   const bool have_forced = tune_lookup(a.level, N, &forced_cfg);
   const TileConfig* forced = have_forced ? &forced_cfg : nullptr;
+  if (a.split) {
+    // split chi: two cells per lane (three or four stencil fields, like COMPLEX)
+    if (N % 2) return cudaErrorNotSupported;
+    // (a tuning recorded for the plain step's tile does not apply)
+    return a.level == LFM_REAL ? plan_and_launch<LFM_REAL, 2, true, kSplit>(P, nullptr, stream)
+                               : plan_and_launch<LFM_COMPLEX, 2, true, kSplit>(P, nullptr, stream);
+  }
   if (a.comp) {
     // compensated Delta form: REAL and COMPLEX, register-queue kernel only
     if (a.level == LFM_REAL)
       return (N % 4) ? cudaErrorNotSupported
-                     : plan_and_launch<LFM_REAL, 4, true, true>(P, forced, stream);
+                     : plan_and_launch<LFM_REAL, 4, true, kComp>(P, forced, stream);
     if (a.level == LFM_COMPLEX)
       return (N % 2) ? cudaErrorNotSupported
-                     : plan_and_launch<LFM_COMPLEX, 2, true, true>(P, forced, stream);
+                     : plan_and_launch<LFM_COMPLEX, 2, true, kComp>(P, forced, stream);
     return cudaErrorNotSupported;
   }
   if (a.level == LFM_REAL) {

@@ -74,6 +74,10 @@ _SIGNATURES = {
     + [_P, _P],
     "lfm_leapfrog_real_comp_f32": [_P] * 7 + [POINTER(MaskLut), c_int] + [_D] * 5 + [_P],
     "lfm_leapfrog_complex_comp_f32": [_P] * 10 + [POINTER(MaskLut), c_int] + [_D] * 6 + [_P],
+    "lfm_leapfrog_real_split_f32": [_P] * 7 + [POINTER(MaskLut), c_int, c_int] + [_D] * 5
+    + [_P],
+    "lfm_leapfrog_complex_split_f32": [_P] * 9 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6
+    + [_P],
     "lfm_helmholtz_sa_f32": [_P] * 4 + [c_int, _D, _D, _P],
     "lfm_sa_clip_f32": [_P, _P, c_int64, _P],
     "lfm_device_status": [POINTER(c_int), c_int],

@@ -2,9 +2,9 @@
 step, and its energy drift.
 
 The workload is the REAL lattice with 64 packets (lfm_b200.workloads.real_solitons:
-chi = 19 +- 1e-3, amplitudes U[2, 6], sigma U[2, 4]).  The plain float32 Evolver
-and the compensated CompensatedEvolver run from the same state as a float64 run
-of the reference step (oracle/torch_ref.py: the reference's NumPy step,
+chi = 19 +- 1e-3, amplitudes U[2, 6], sigma U[2, 4]).  The plain float32 Evolver,
+the compensated CompensatedEvolver and the split-chi SplitChiEvolver run from the
+same state as a float64 run of the reference step (oracle/torch_ref.py: the reference's NumPy step,
 transcribed to torch, in float64 on the GPU).
 
 * Error: max-relative, max|x - x64| / max|x64|, for E and chi.
@@ -76,6 +76,7 @@ def accuracy_report(N: int, steps: int, device: str = "cuda:0") -> dict:
     from lfm_b200.compensated import CompensatedEvolver
     from lfm_b200.config import gravity_only
     from lfm_b200.mask import boundary_mask
+    from lfm_b200.split import SplitChiEvolver
     from lfm_b200.workloads import real_solitons
     from oracle import torch_ref as TR
 
@@ -96,7 +97,8 @@ def accuracy_report(N: int, steps: int, device: str = "cuda:0") -> dict:
     out["fp64"] = {"energy_0": E0, "energy_T": E1, "drift_percent": abs(E1 - E0) / abs(E0) * 100}
 
     be = B200Backend(device)
-    for name, cls in (("plain_f32", Evolver), ("compensated_f32", CompensatedEvolver)):
+    for name, cls in (("plain_f32", Evolver), ("compensated_f32", CompensatedEvolver),
+                      ("split_f32", SplitChiEvolver)):
         ev = cls(cfg, backend=be)
         ev.set_psi_real(E)
         ev.set_chi(chi)
@@ -108,7 +110,7 @@ def accuracy_report(N: int, steps: int, device: str = "cuda:0") -> dict:
         ch = st["chi"].view(N, N, N)
         out[name] = {
             "max_rel_error_E": max_rel(pr, s["pr"]),
-            "max_rel_error_chi": max_rel(ch, s["chi"]),
+            "max_rel_error_chi": max_rel(st.get("chi64", ch).view(N, N, N), s["chi"]),
             "energy_0": m0, "energy_T": m1,
             "drift_percent": abs(m1 - m0) / abs(m0) * 100,
             # the device reduction against energy64 on the same float32 state
@@ -175,7 +177,7 @@ def test_accuracy_and_energy_drift_of_the_throughput_workload(cuda_device):
     reduction agrees with the float64 restatement of energy.py."""
     r = accuracy_report(64, 200, cuda_device)
     print(json.dumps(r, indent=1))
-    for name in ("plain_f32", "compensated_f32"):
+    for name in ("plain_f32", "compensated_f32", "split_f32"):
         p = r[name]
         assert p["energy_T"] == pytest.approx(p["energy_T_energy64"], rel=1e-9), name
         # measured: E 2.6e-4 (compensated), chi 1.1e-4 (plain) / 5.2e-5 (compensated),
@@ -184,6 +186,7 @@ def test_accuracy_and_energy_drift_of_the_throughput_workload(cuda_device):
         assert p["max_rel_error_chi"] < 5e-4, name
         assert abs(p["drift_minus_fp64_drift"]) < 1e-3, name  # percentage points
     assert r["compensated_f32"]["max_rel_error_chi"] <= r["plain_f32"]["max_rel_error_chi"]
+    assert r["split_f32"]["max_rel_error_E"] < 1e-5 and r["split_f32"]["max_rel_error_chi"] < 1e-6
 
 
 if __name__ == "__main__":

@@ -49,6 +49,8 @@ TOL = {
     # config 1, 1000 steps: plain float32 E 8.8e-3, chi 5.2e-4; compensated 4.0e-3, 9.7e-5
     "c1_plain_E": 1.5e-2, "c1_plain_chi": 8e-4,
     "c1_comp_E": 6e-3, "c1_comp_chi": 1.5e-4,
+    # split chi: the north-star bound itself (CPU emulation before the kernel: 3.9e-6, 4.7e-8)
+    "split_E": 1e-5, "split_chi": 1e-6,
     # config 2, 2000 steps: plain E 1.1e-1, chi 1.6e-3; compensated 4.8e-3, 1.5e-4
     "c2_plain_E": 0.17, "c2_plain_chi": 2.5e-3,
     "c2_comp_E": 7.5e-3, "c2_comp_chi": 2.5e-4,
@@ -103,6 +105,7 @@ def test_config1_real64_1000_steps(be):
     from lfm_b200.compensated import CompensatedEvolver
     from lfm_b200.config import gravity_only
     from lfm_b200.metrics import interior_mask
+    from lfm_b200.split import SplitChiEvolver
     from lfm_b200.workloads import config1_soliton
 
     N, steps = 64, 1000
@@ -128,7 +131,8 @@ def test_config1_real64_1000_steps(be):
     out = {"N": N, "steps": steps, "workload": "REAL gravity_only, packet 6.0 sigma 3 + 1e-4 noise"}
     cmin, wf = _chi_stats(ref["chi"], interior)
     out["fp64"] = {"chi_min": cmin, "well_fraction": wf}
-    for name, cls in (("plain_f32", Evolver), ("compensated_f32", CompensatedEvolver)):
+    for name, cls in (("plain_f32", Evolver), ("compensated_f32", CompensatedEvolver),
+                      ("split_f32", SplitChiEvolver)):
         ev = cls(cfg, backend=be)
         ev.set_psi_real(E)
         ev.evolve(steps)
@@ -137,7 +141,8 @@ def test_config1_real64_1000_steps(be):
         m = ev.metrics()
         cmin32, wf32 = _chi_stats(chi, interior)
         out[name] = {"max_rel_error_E": max_rel(pr, ref["pr"]),
-                     "max_rel_error_chi": max_rel(chi, ref["chi"]),
+                     "max_rel_error_chi": max_rel(st.get("chi64", chi).view(N, N, N),
+                                                  ref["chi"]),
                      "chi_min": m["chi_min"], "chi_min_interior_check": cmin32,
                      "well_fraction": m["well_fraction"], "well_fraction_check": wf32}
     # sensitivity of the float64 run itself
@@ -160,11 +165,13 @@ def test_config1_real64_1000_steps(be):
     out["fp64_sensitivity"] = sens
     record("config1_real64_1000", out)
 
-    p, c = out["plain_f32"], out["compensated_f32"]
+    p, c, sp = out["plain_f32"], out["compensated_f32"], out["split_f32"]
     assert p["max_rel_error_E"] < TOL["c1_plain_E"] and p["max_rel_error_chi"] < TOL["c1_plain_chi"]
     assert c["max_rel_error_E"] < TOL["c1_comp_E"] and c["max_rel_error_chi"] < TOL["c1_comp_chi"]
     assert c["max_rel_error_chi"] < p["max_rel_error_chi"]
-    for r in (p, c):
+    # within 1e-5 of float64 after 1000 float32-stored steps
+    assert sp["max_rel_error_E"] < TOL["split_E"] and sp["max_rel_error_chi"] < TOL["split_chi"]
+    for r in (p, c, sp):
         assert r["chi_min"] == r["chi_min_interior_check"]
         assert r["well_fraction"] == pytest.approx(r["well_fraction_check"], abs=1e-12)
         assert abs(r["chi_min"] - cmin) < 1e-3 * abs(cmin)
