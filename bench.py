@@ -199,6 +199,26 @@ def cpu_baseline(N: int, seconds: float, E, chi) -> dict:
                       f"({el:.1f} s, {threads} threads of {os.cpu_count()})"}
 
 
+def cpu_baseline_numpy(N: int, E, chi) -> dict:
+    """The reference's CPU path as its NumPy whole-array operations (one core, as
+    NumPy runs them): one REAL step of the whole lattice."""
+    from lfm_b200.config import gravity_only
+    from lfm_b200.mask import boundary_mask
+    from oracle import oracle as O
+
+    cfg = gravity_only(N)
+    mask = boundary_mask(N, cfg.boundary_fraction)
+    Ef, chif = E.reshape(-1), chi.reshape(-1)
+    t0 = time.perf_counter()
+    O.numpy_step_real(Ef, Ef, chif, chif, mask, N, cfg.dt**2, cfg.kappa, cfg.lambda_self,
+                      cfg.chi0, cfg.e0_sq)
+    el = time.perf_counter() - t0
+    return {"value": N**3 / el / 1e9, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"one REAL step of the whole {N}^3 lattice with the reference's NumPy "
+                      f"array operations (oracle.numpy_step_real, bit-exact to the reference; "
+                      f"{el:.1f} s, single-threaded NumPy)"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -699,6 +719,7 @@ def run_b200(args):
         line["color"] = color
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(N, args.cpu_seconds, E, chi)
+        line["cpu_baseline_numpy"] = cpu_baseline_numpy(N, E, chi)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

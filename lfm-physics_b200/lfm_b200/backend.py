@@ -19,6 +19,28 @@ from . import _lib
 from .mask import boundary_mask as _host_mask
 
 
+_DEVICE_ARRAY = None
+
+
+def device_array(t):
+    """`t` as a DeviceArray: a torch tensor that also has NumPy/CuPy's ``copy()``.
+
+    The reference Evolver snapshots its chi buffers with ``.copy()`` when it
+    evolves with freeze_chi (lfm/core/evolver.py:160-166), which torch tensors
+    spell ``clone()``; every array this backend hands out answers both.
+    """
+    global _DEVICE_ARRAY
+    if _DEVICE_ARRAY is None:
+        import torch
+
+        class DeviceArray(torch.Tensor):
+            def copy(self):
+                return self.clone()
+
+        _DEVICE_ARRAY = DeviceArray
+    return t.as_subclass(_DEVICE_ARRAY)
+
+
 def _stream_handle(device) -> int:
     import torch
 
@@ -81,10 +103,11 @@ class B200Backend:
         z = lambda n: torch.zeros(n, dtype=torch.float32, device=self.device)  # noqa: E731
         f = lambda n: torch.full((n,), float(chi0), dtype=torch.float32, device=self.device)  # noqa: E731
         psi = n_psi_arrays * total
-        return {
+        out = {
             "psi_A": z(psi), "psi_prev_A": z(psi), "chi_A": f(total), "chi_prev_A": f(total),
             "psi_B": z(psi), "psi_prev_B": z(psi), "chi_B": f(total), "chi_prev_B": f(total),
         }
+        return {k: device_array(v) for k, v in out.items()}
 
     def create_boundary_mask(self, N: int, boundary_fraction: float):
         return self.from_numpy(_host_mask(N, boundary_fraction))
@@ -97,7 +120,8 @@ class B200Backend:
     def from_numpy(self, arr):
         import torch
 
-        return torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(self.device)
+        return device_array(
+            torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float32)).to(self.device))
 
     def synchronize(self) -> None:
         import torch

@@ -15,6 +15,8 @@ Contents
   the reference ``Backend`` signatures (lfm/core/backends/protocol.py:65-136),
   computed by the C restatement in ``lfm_oracle.cpp`` (float32: bit-exact to
   NumPy's float32 path; float64: the FP64 oracle).
+* ``numpy_step_real`` -- the REAL step as the reference's NumPy whole-array
+  operations (one core), the timed stand-in for the reference's CPU path.
 * ``gaussian_soliton`` / ``equilibrate_chi`` / ``interior_mask`` -- the
   packet builder and the Poisson equilibration of lfm/fields/soliton.py and
   lfm/fields/equilibrium.py (NumPy restatements).
@@ -196,6 +198,54 @@ def laplacian_19pt(field: np.ndarray) -> np.ndarray:
     out = np.empty_like(f)
     getattr(_load(), f"oracle_laplacian_{_dtype_suffix(f)}")(f.ravel(), out.ravel(), N)
     return out
+
+
+# --------------------------------------------------------------------------
+# the reference's CPU path as NumPy whole-array operations (for timing)
+# --------------------------------------------------------------------------
+# Neighbour offsets of the 19-point stencil in the order the reference sums
+# them (lfm/core/stencils.py:43-71): np.roll(f, s, axis) is the f[x - s]
+# neighbour; faces first, then the xy, xz and yz edges.
+_FACE_ROLLS = ((1, 0), (-1, 0), (1, 1), (-1, 1), (1, 2), (-1, 2))
+_EDGE_ROLLS = tuple(((s, a), (t, b)) for a, b in ((0, 1), (0, 2), (1, 2))
+                    for s in (1, -1) for t in (1, -1))
+
+
+def numpy_laplacian(f: np.ndarray) -> np.ndarray:
+    """The 19-point Laplacian as the reference's NumPy code evaluates it: one rolled
+    temporary per neighbour, summed left to right, then the three weightings."""
+    faces = None
+    for s, a in _FACE_ROLLS:
+        t = np.roll(f, s, axis=a)
+        faces = t if faces is None else faces + t
+    edges = None
+    for (s, a), (t_, b) in _EDGE_ROLLS:
+        t = np.roll(np.roll(f, s, axis=a), t_, axis=b)
+        edges = t if edges is None else edges + t
+    return (1.0 / 3.0) * faces + (1.0 / 6.0) * edges + (-4.0) * f
+
+
+def numpy_step_real(E, E_prev, chi, chi_prev, mask, N, dt2, kappa, lambda_self, chi0,
+                    e0_sq):
+    """One REAL step with NumPy whole-array operations, single-threaded, in the
+    reference's order (numpy_backend.py:80-130).  Returns (E', E_prev', chi', chi_prev').
+    bench.py times it as the reference's own CPU path; tests pin it to the C oracle."""
+    shape = (N, N, N)
+    E, E_prev, chi, chi_prev, mask = (np.asarray(a).reshape(shape)
+                                      for a in (E, E_prev, chi, chi_prev, mask))
+    lap_e = numpy_laplacian(E)
+    lap_x = numpy_laplacian(chi)
+    chi_sq = chi * chi
+    e_new = 2.0 * E - E_prev + dt2 * (lap_e - chi_sq * E)
+    acc = lap_x - (kappa / chi0) * chi * (E * E - e0_sq)
+    if lambda_self > 0:
+        acc -= 4.0 * lambda_self * chi * (chi_sq - chi0 * chi0)
+    chi_new = 2.0 * chi - chi_prev + dt2 * acc
+    np.clip(chi_new, -chi0, None, out=chi_new)
+    absorb = 1.0 - mask
+    e_new *= absorb
+    chi_new = mask * chi0 + absorb * chi_new
+    return e_new.ravel(), (E * absorb).ravel(), chi_new.ravel(), chi.ravel().copy()
 
 
 # --------------------------------------------------------------------------

@@ -81,6 +81,18 @@ def test_single_step_real_bit_exact(N):
 
 
 @pytest.mark.parametrize("N", [12, 13])
+def test_numpy_restatement_of_the_real_step_bit_exact(N):
+    """numpy_step_real (the reference's CPU path as NumPy array operations, timed by
+    bench.py as the single-core reference baseline) reproduces the reference's step."""
+    g = load_golden("single_step.npz")
+    ins = [g[f"real{N}_in_{k}"] for k in ("E", "Ep", "chi", "chip")]
+    outs = O.numpy_step_real(*ins, O.boundary_mask(N, 0.3), N, DT2, KAPPA, LAMBDA_H, CHI0, 0.0)
+    for k, a in zip(("E", "Ep", "chi", "chip"), outs):
+        assert a.dtype == np.float32
+        assert np.array_equal(a, g[f"real{N}_out_{k}"]), k
+
+
+@pytest.mark.parametrize("N", [12, 13])
 def test_single_step_complex_bit_exact(N):
     g = load_golden("single_step.npz")
     names = ("Pr", "Prp", "Pi", "Pip", "chi", "chip")
