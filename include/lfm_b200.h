@@ -403,6 +403,15 @@ int lfm_metrics_f64_noalloc(int level, const float* psi_r, const float* psi_r_pr
                             double well_threshold, double void_threshold, double* out_host,
                             void* stream);
 
+/* Transform of the S_a solve (no counterpart in the reference, which always
+ * runs 3-D FFTs): 1 = split (default): 2-D cuFFT transforms over (j, k) and
+ * one hand-written pass along i that does the forward FFT, the Helmholtz
+ * filter and the inverse FFT (N in {64, 128, 256, 512, 1024}; other N use the
+ * 3-D path); 0 = 3-D cuFFT transforms with a separate filter pass.  Both
+ * follow numpy_backend.py:341-356 and agree to float32 rounding.
+ * Process-wide; for tests and tuning. */
+int lfm_set_sa_transform(int mode);
+
 /* Kernel path for the step calls: 0 = automatic (fused 2.5D kernel where
  * it applies, the direct kernel otherwise), 1 = direct kernel only,
  * 2 = fused kernel only (calls it cannot serve return LFM_ERR_UNSUPPORTED).

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <climits>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -55,6 +56,9 @@ int cuda_fail(cudaError_t e, const char* what) {
 // Kernel path: 0 = choose (fused 2.5D kernel when it applies), 1 = direct
 // kernel only, 2 = fused kernel only (LFM_ERR_UNSUPPORTED when it cannot run).
 std::atomic<int> g_path{0};
+// S_a transform: 1 = split (2-D cuFFT + fused pass along i) where N allows it,
+// 0 = 3-D cuFFT with a separate filter pass.  Process-wide; for tests.
+std::atomic<int> g_sa_split{1};
 
 constexpr int kMaxDevices = 64;
 std::mutex g_status_mu;
@@ -160,6 +164,11 @@ struct FftSlot {
   cufftHandle r2c = 0, c2r = 0;
   float2* spec = nullptr;   // 3 * N * N * (N/2+1) complex
   float* sa_raw = nullptr;  // 3 * N^3, for protocol colour steps
+  // Split transform (power-of-two N, spectral.cu): 2-D transforms over (j, k)
+  // for every plane and colour, the pass along i fused with the filter.
+  cufftHandle r2c_2d = 0, c2r_2d = 0;
+  float2* twiddles = nullptr;                              // e^{-2 pi i t / N}, t < N
+  std::map<std::pair<double, double>, float*> tables;      // filter per (gamma, D)
 };
 
 // Poisson equilibration scratch per lattice edge: float32 R2C of the
@@ -234,6 +243,56 @@ int poisson_slot(lfm_context* ctx, int N, PoissonSlot** out) {
   return LFM_OK;
 }
 
+// The split transform's plans, twiddles and the filter table for (gamma, D),
+// created on first use (outside stream capture: they allocate and upload).
+int split_transform(FftSlot* s, int N, double gamma, double d, cudaStream_t stream,
+                    float** table) {
+  const std::pair<double, double> key(gamma, d);
+  auto it = s->tables.find(key);
+  if (s->r2c_2d && it != s->tables.end()) {
+    *table = it->second;
+    return LFM_OK;
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(LFM_ERR_UNSUPPORTED,
+                "the first S_a solve for N=%d, gamma=%g, D=%g must run outside stream capture",
+                N, gamma, d);
+  const int nz = N / 2 + 1;
+  if (!s->r2c_2d) {
+    int n[2] = {N, N}, inr[2] = {N, N}, inc[2] = {N, nz};
+    if (cufftPlanMany(&s->r2c_2d, 2, n, inr, 1, N * N, inc, 1, N * nz, CUFFT_R2C, 3 * N) !=
+        CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlanMany 2-D R2C N=%d", N);
+    if (cufftPlanMany(&s->c2r_2d, 2, n, inc, 1, N * nz, inr, 1, N * N, CUFFT_C2R, 3 * N) !=
+        CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftPlanMany 2-D C2R N=%d", N);
+    std::vector<float2> tw(N);
+    for (int t = 0; t < N; ++t) {
+      const double ang = -2.0 * 3.14159265358979323846 * (double)t / (double)N;
+      tw[t] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    e = cudaMalloc(&s->twiddles, sizeof(float2) * N);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(s->twiddles, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
+  }
+  float* t = nullptr;
+  e = cudaMalloc(&t, sizeof(float) * (size_t)nz * nz * nz);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc filter table");
+  e = lfm::launch_helmholtz_table(t, N, gamma, d, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    cudaFree(t);
+    return cuda_fail(e, "filter table");
+  }
+  s->tables[key] = t;
+  *table = t;
+  return LFM_OK;
+}
+
 int helmholtz(lfm_context* ctx, const float* pr, const float* pi, float* sa_raw, int N,
               double gamma, double d, cudaStream_t stream, bool use_ctx_scratch,
               float** sa_used) {
@@ -244,6 +303,21 @@ int helmholtz(lfm_context* ctx, const float* pr, const float* pi, float* sa_raw,
   float* dst = use_ctx_scratch ? s->sa_raw : sa_raw;
   cudaError_t e = lfm::launch_color_energy(pr, pi, dst, N, stream);
   if (e != cudaSuccess) return cuda_fail(e, "|Psi_a|^2 launch");
+  if (lfm::helmholtz_xpass_supported(N) && g_sa_split.load()) {
+    float* table = nullptr;
+    rc = split_transform(s, N, gamma, d, stream, &table);
+    if (rc) return rc;
+    if (cufftSetStream(s->r2c_2d, stream) != CUFFT_SUCCESS ||
+        cufftExecR2C(s->r2c_2d, dst, reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftExecR2C 2-D N=%d", N);
+    e = lfm::launch_helmholtz_xpass(s->spec, table, s->twiddles, N, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "Helmholtz pass along i");
+    if (cufftSetStream(s->c2r_2d, stream) != CUFFT_SUCCESS ||
+        cufftExecC2R(s->c2r_2d, reinterpret_cast<cufftComplex*>(s->spec), dst) != CUFFT_SUCCESS)
+      return fail(LFM_ERR_CUFFT, "cufftExecC2R 2-D N=%d", N);
+    if (sa_used) *sa_used = dst;
+    return LFM_OK;
+  }
   if (cufftSetStream(s->r2c, stream) != CUFFT_SUCCESS ||
       cufftExecR2C(s->r2c, dst, reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
     return fail(LFM_ERR_CUFFT, "cufftExecR2C N=%d", N);
@@ -279,6 +353,12 @@ const char* lfm_strerror(int status) {
 const char* lfm_last_error_detail(void) { return t_detail.c_str(); }
 
 int lfm_abi_version(void) { return LFM_B200_ABI_VERSION; }
+
+int lfm_set_sa_transform(int mode) {
+  if (mode < 0 || mode > 1) return fail(LFM_ERR_INVALID_ARG, "mode %d not in {0,1}", mode);
+  g_sa_split.store(mode);
+  return LFM_OK;
+}
 
 int lfm_set_step_path(int path) {
   if (path < 0 || path > 2) return fail(LFM_ERR_INVALID_ARG, "path %d not in {0,1,2}", path);
@@ -476,8 +556,12 @@ int lfm_context_destroy(lfm_context* ctx) {
   for (auto& kv : ctx->slots) {
     if (kv.second.r2c) cufftDestroy(kv.second.r2c);
     if (kv.second.c2r) cufftDestroy(kv.second.c2r);
+    if (kv.second.r2c_2d) cufftDestroy(kv.second.r2c_2d);
+    if (kv.second.c2r_2d) cufftDestroy(kv.second.c2r_2d);
     if (kv.second.spec) cudaFree(kv.second.spec);
     if (kv.second.sa_raw) cudaFree(kv.second.sa_raw);
+    if (kv.second.twiddles) cudaFree(kv.second.twiddles);
+    for (auto& t : kv.second.tables) cudaFree(t.second);
   }
   for (auto& kv : ctx->poisson) {
     PoissonSlot& p = kv.second;

@@ -66,6 +66,13 @@ cudaError_t launch_color_energy(const float* pr, const float* pi, float* e, int 
 cudaError_t launch_helmholtz_multiply_gd(float2* spec, int N, double gamma, double d,
                                          cudaStream_t stream);
 cudaError_t launch_clip(const float* in, float* out, int64_t count, cudaStream_t stream);
+// The split S_a transform (spectral.cu): which N it serves, the filter table
+// ((N/2+1)^3 floats) and the fused pass along i on spec[3][N][N*(N/2+1)].
+bool helmholtz_xpass_supported(int N);
+cudaError_t launch_helmholtz_table(float* table, int N, double gamma, double d,
+                                   cudaStream_t stream);
+cudaError_t launch_helmholtz_xpass(float2* spec, const float* table, const float2* twiddles,
+                                   int N, cudaStream_t stream);
 
 // Poisson equilibration pieces (poisson.cu).
 cudaError_t launch_poisson_rhs(const float* pr, const float* pi, float* rhs, int N, int colours,

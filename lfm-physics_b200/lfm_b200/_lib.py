@@ -62,6 +62,7 @@ _D = c_double
 _SIGNATURES = {
     "lfm_abi_version": [],
     "lfm_set_step_path": [c_int],
+    "lfm_set_sa_transform": [c_int],
     "lfm_mask_lut_build": [c_int, _P, _P, c_int, POINTER(MaskLut)],
     "lfm_step_real_f32": [_P] * 9 + [c_int] + [_D] * 5 + [_P],
     "lfm_step_complex_f32": [_P] * 13 + [c_int] + [_D] * 6 + [_P],
