@@ -15,8 +15,15 @@ initial state copied from pinned host memory and the final fields copied
 back inside the timed region.  --impl reference times the CPU oracle (the
 bit-exact restatement of the reference NumPy path) on the host cores.
 
-Multi-GPU (torchrun): every rank evolves its own lattice (independent
-lattices, no collective in the data path): weak scaling.
+Multi-GPU (torchrun), --mode:
+  replicas (default)  every rank evolves its own lattice (independent lattices,
+                      no collective in the data path): weak scaling;
+  slab                one lattice split along i, one slab per rank, the ghost
+                      planes exchanged with NCCL point-to-point after every step
+                      (overlapped with the interior planes): strong scaling;
+  sweep               the batched-sweep lattices shared out over the ranks by cost,
+                      one batched launch per step on each, no collective while
+                      stepping: strong scaling.
 """
 
 from __future__ import annotations
@@ -46,6 +53,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--mode", choices=["replicas", "slab", "sweep"], default="replicas",
+                    help="replicas: every rank evolves its own lattice (weak scaling, the "
+                         "default); slab: one lattice split along i over the ranks with the "
+                         "NCCL ghost exchange (strong scaling); sweep: the batched-sweep "
+                         "lattices split over the ranks (strong scaling)")
     ap.add_argument("--N", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="approximate CPU time of the oracle baseline sample")
@@ -352,6 +364,17 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
 
     ms_p = timed(plain)
     del evs
+
+    # The loop as the reference's sweep runs it (sweep.py:52-82): per value a fresh
+    # simulation object, its state set from the host, the steps, the metrics at the end.
+    def reference_semantics():
+        for c, pr, pi in L:
+            ev = Evolver(c, backend=be)
+            load(ev, 0, pr, pi)
+            ev.evolve(steps)
+            ev.metrics()
+
+    ms_r = timed(reference_semantics)
     vb = cells * steps / (ms_b / 1e3) / 1e9
     vp = cells * steps / (ms_p / 1e3) / 1e9
     ach = bytes_step * steps / (ms_b / 1e3) / 1e9
@@ -363,6 +386,11 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
                            "how": "one Evolver per lattice, evolve(steps) each in turn "
                                   "(two-step CUDA graphs)"},
             "speedup_vs_plain_loop": ms_p / ms_b,
+            "reference_semantics_loop": {
+                "value": cells * steps / (ms_r / 1e3) / 1e9, "unit": METRIC, "ms": ms_r,
+                "how": "per lattice: a new Evolver, its state from the host, evolve(steps), "
+                       "metrics() (the reference sweep's per-value loop, sweep.py:52-82)"},
+            "speedup_vs_reference_semantics_loop": ms_r / ms_b,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "bytes_per_cell": "24 REAL / 36 COMPLEX"},
             "launch": info, "gpu_launches": steps,
@@ -728,10 +756,153 @@ def run_b200(args):
     return 0
 
 
+def _dist_setup():
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return rank, world, dev, barrier, max_over_ranks
+
+
+def _common_line(args, value, ms, world, config, scaling, clock_info, launches):
+    return {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": scaling, "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config, "clocks": clock_info,
+            "gpu_launches": launches}
+
+
+def run_slab(args):
+    """One REAL N^3 lattice split along i over the ranks (SlabEvolver)."""
+    import torch
+    import torch.distributed as dist
+
+    from lfm_b200 import B200Backend, _lib
+    from lfm_b200.config import gravity_only
+    from lfm_b200.slab import SlabEvolver
+    from lfm_b200.workloads import real_solitons
+
+    rank, world, dev, barrier, max_over_ranks = _dist_setup()
+    N = args.N
+    E, chi = real_solitons(N)
+    s = SlabEvolver(gravity_only(N), backend=B200Backend(dev))
+    s.set_psi_real(E)
+    s.set_chi(chi)
+    s.evolve(max(args.warmup, 3))
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(int(dev.index))
+    barrier()
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    s.evolve(args.steps)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clock_info = clocks.stop()
+    ms = max_over_ranks(a.elapsed_time(b))
+    status = _lib.device_status(clear=True)
+    if status:
+        raise RuntimeError(f"device status word {status} after the slab steps")
+    overlapped = world > 1 and s.n_local >= 3
+    cfg = dict(workload_config(N, "real"), parallelism=f"slab x{world} along i",
+               planes_per_rank=s.n_local, overlap=overlapped,
+               exchange_bytes_per_rank_step=0 if world == 1 else 2 * 2 * N * N * 4,
+               l2="inputs > L2, no flush")
+    line = _common_line(args, N**3 * args.steps / (ms / 1e3) / 1e9, ms, world, cfg, "strong",
+                        clock_info, args.steps * (3 if overlapped else 1))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_sweep_sharded(args):
+    """The batched-sweep lattices shared out over the ranks by cost (lfm_b200.sweep.shard);
+    each rank advances its share in one batched launch per step."""
+    import torch
+    import torch.distributed as dist
+
+    from lfm_b200 import B200Backend, _lib
+    from lfm_b200.batch import BatchedLattices
+    from lfm_b200.sweep import shard
+    from lfm_b200.workloads import sweep_lattices
+
+    rank, world, dev, barrier, max_over_ranks = _dist_setup()
+    L = sweep_lattices(args.batch_lattices, seed=5)
+    parts = shard([c.grid_size**3 for c, _, _ in L], world)
+    mine = [L[i] for i in parts[rank]]
+    steps = args.steps + (args.steps % 2)
+    B = BatchedLattices([c for c, _, _ in mine], backend=B200Backend(dev))
+    B.graph_block = steps
+    for i, (c, pr, pi) in enumerate(mine):
+        B.set_psi_real(i, pr)
+        if pi is not None:
+            B.set_psi_imag(i, pi)
+    B.evolve(max(args.warmup, 3) | 1)
+    B.evolve(steps)
+    B.evolve(steps)
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    clocks = ClockSampler(int(dev.index))
+    barrier()
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    B.evolve(steps)
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    clock_info = clocks.stop()
+    ms = max_over_ranks(a.elapsed_time(b))
+    status = _lib.device_status(clear=True)
+    if status:
+        raise RuntimeError(f"device status word {status} after the sharded sweep")
+    cells = sum(c.grid_size**3 for c, _, _ in L)
+    cfg = {"workload": f"batched sweep: {len(L)} lattices, N in {{32..96}}, REAL/COMPLEX mixed",
+           "lattices": len(L), "cells": cells, "parallelism": f"lattices sharded x{world}",
+           "lattices_this_rank0": len(parts[0]), "l2": "every lattice stepped once per step"}
+    line = _common_line(args, cells * steps / (ms / 1e3) / 1e9, ms, world, cfg, "strong",
+                        clock_info, steps)
+    line["steps"] = steps
+    del B
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "slab":
+        return run_slab(args)
+    if args.mode == "sweep":
+        return run_sweep_sharded(args)
     return run_b200(args)
 
 

@@ -228,9 +228,11 @@ def numpy_laplacian(f: np.ndarray) -> np.ndarray:
 def numpy_step_real(E, E_prev, chi, chi_prev, mask, N, dt2, kappa, lambda_self, chi0,
                     e0_sq):
     """One REAL step with NumPy whole-array operations, single-threaded, in the
-    reference's order (numpy_backend.py:80-130).  Returns (E', E_prev', chi', chi_prev').
-    bench.py times it as the reference's own CPU path; tests pin it to the C oracle."""
-    shape = (N, N, N)
+    reference's order (numpy_backend.py:80-130).  Returns (E', E_prev', chi', chi_prev'),
+    flat.  bench.py times it as the reference's own CPU path; tests pin it to the C oracle.
+    Fields given as (P, N, N) arrays step as P planes wrapped in i (a slab with its
+    ghost planes: its inner planes come out as the whole lattice's)."""
+    shape = np.shape(E) if np.ndim(E) == 3 else (N, N, N)
     E, E_prev, chi, chi_prev, mask = (np.asarray(a).reshape(shape)
                                       for a in (E, E_prev, chi, chi_prev, mask))
     lap_e = numpy_laplacian(E)

@@ -108,6 +108,80 @@ def test_ghost_exchange_over_gloo_matches_the_whole_lattice(world, N, cx, overla
             assert np.array_equal(pi, want["psi_i"]), rank
 
 
+# The reference's REAL step (oracle.numpy_step_real, pinned to the reference's
+# fixtures) on a slab's planes with their ghosts: what lfm_slab_step_planes_f32
+# computes on the GPU, here on the CPU, so the gloo ranks run the slab plan
+# (plane ranges, ghost planes, damping of the previous field on read) with the
+# step's own arithmetic.
+def oracle_slab_step(slab, lo, hi):
+    import torch
+
+    from lfm_b200.mask import boundary_mask
+    from oracle import oracle as O
+
+    N, cfg = slab.N, slab.config
+    c, p = slab.cur, 1 - slab.cur
+    m = boundary_mask(N, cfg.boundary_fraction).reshape(N, N, N)[slab._global_planes()]
+    e, x = slab.pr[c].numpy(), slab.chi[c].numpy()
+    ep, xp = slab.pr[p].numpy(), slab.chi[p].numpy()
+    if slab.damp:  # the previous slot holds the undamped field
+        ep = ep * (np.float32(1.0) - m)
+    out = O.numpy_step_real(e, ep, x, xp, m, N, cfg.dt**2, cfg.kappa, cfg.lambda_self,
+                            cfg.chi0, cfg.e0_sq)
+    shape = e.shape
+    slab.pr[p][lo:hi] = torch.from_numpy(out[0].reshape(shape)[lo:hi])
+    slab.chi[p][lo:hi] = torch.from_numpy(out[2].reshape(shape)[lo:hi])
+
+
+def _gloo_oracle_worker(rank, world, port, N, overlap, q):
+    import torch.distributed as dist
+
+    from lfm_b200.slab import SlabEvolver
+    from lfm_b200.workloads import config1_soliton
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        s = SlabEvolver(_cfg(N, False), stepper=oracle_slab_step, device="cpu")
+        s.overlap = overlap
+        s.set_psi_real(config1_soliton(N))
+        s.evolve(6)
+        q.put((rank, s.get_psi_real(), s.get_chi()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world, N, overlap", [(2, 16, True), (3, 16, True), (2, 12, False)])
+def test_slab_plan_with_the_real_step_over_gloo_is_bit_exact(world, N, overlap):
+    """Every rank steps its slab with the reference's arithmetic (boundary planes, the
+    exchange, then the interior with overlap); the gathered lattice equals the oracle's
+    whole-lattice steps bit for bit."""
+    import torch.multiprocessing as mp
+
+    from lfm_b200.workloads import config1_soliton
+    from oracle import oracle as O
+
+    lat = O.OracleLattice(_cfg(N, False))
+    lat.set_psi_real(config1_soliton(N))
+    lat.step(6)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gloo_oracle_worker, args=(r, world, port, N, overlap, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, pr, chi in got:
+        assert bits_equal(pr.ravel(), lat.pr), rank
+        assert bits_equal(chi.ravel(), lat.chi), rank
+
+
 def test_slab_rejects_color():
     from lfm_b200.config import full_physics
     from lfm_b200.slab import SlabEvolver
