@@ -162,6 +162,21 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
                            double kappa_string, double kappa_tube, const float* sa,
                            void* stream);
 
+/* lfm_leapfrog_color_f32 that also writes |Psi_a|^2 = Pr_a^2 + Pi_a^2 of the
+ * new fields (as stored) to energy_out (3 N^3 floats, distinct from every
+ * other buffer; NULL: not written), in the step kernel's epilogue.  The next
+ * step's S_a solve then starts from it (lfm_helmholtz_sa_from_energy_f32)
+ * instead of reading all six Psi arrays again: the same bits as the
+ * |Psi_a|^2 lfm_helmholtz_sa_f32 forms (numpy_backend.py:289). */
+int lfm_leapfrog_color_energy_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                                  float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                                  const float* mask_table, const lfm_mask_lut* lut,
+                                  int damp_prev, int N, double dt2, double kappa,
+                                  double lambda_self, double chi0, double e0_sq,
+                                  double epsilon_w, double kappa_c, double epsilon_cc,
+                                  double kappa_string, double kappa_tube, const float* sa,
+                                  float* energy_out, void* stream);
+
 /* ------------------------------------------------------------------------
  * Compensated float32 steps (Delta form).  No counterpart kernel in the
  * reference; they advance the same equations as lfm_leapfrog_real_f32 /
@@ -354,13 +369,23 @@ int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_
 /* ------------------------------------------------------------------------
  * S_a Helmholtz solve (numpy_backend.py:341-356, cupy_backend.py:261-279):
  * sa_raw[a] = IRFFT[ gamma/(gamma + D|k|^2) * RFFT(|Psi_a|^2) ] for a = 0..2,
- * k = 2*pi*fftfreq(N), computed in float32 with cuFFT (R2C, hand-written
- * k-space multiply with 1/N^3 folded in, C2R).  sa_raw is NOT clipped;
- * consumers clip at 0 (lfm_sa_clip_f32 for a host-visible copy).
+ * k = 2*pi*fftfreq(N), computed in float32.  N in {64, 128, 256, 512, 1024}:
+ * cuFFT 2-D R2C over (j, k) per plane, one hand-written pass along i (forward
+ * FFT, the filter with 1/N^3 folded in, inverse FFT), cuFFT 2-D C2R; other N:
+ * cuFFT 3-D R2C, a hand-written k-space multiply, 3-D C2R
+ * (lfm_set_sa_transform).  sa_raw is NOT clipped; consumers clip at 0
+ * (lfm_sa_clip_f32 for a host-visible copy).
  * ------------------------------------------------------------------------ */
 int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
                          float* sa_raw, int N, double sa_gamma, double sa_d, void* stream);
 int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* stream);
+
+/* The S_a solve of lfm_helmholtz_sa_f32 from |Psi_a|^2 already at hand
+ * (energy: 3 N^3 floats, e.g. from lfm_leapfrog_color_energy_f32), skipping
+ * the pass that forms it from psi_r and psi_i.  The energy array is consumed:
+ * its contents are undefined afterwards. */
+int lfm_helmholtz_sa_from_energy_f32(lfm_context* ctx, const float* energy, float* sa_raw,
+                                     int N, double sa_gamma, double sa_d, void* stream);
 
 /* ------------------------------------------------------------------------
  * Float64 metrics of a state, reduced on the device (replaces the host

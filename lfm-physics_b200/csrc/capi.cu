@@ -293,22 +293,30 @@ int split_transform(FftSlot* s, int N, double gamma, double d, cudaStream_t stre
   return LFM_OK;
 }
 
+// S_a from |Psi_a|^2: from pr, pi (the energy is formed first, into the
+// output buffer), or from a given energy array (pr == pi == nullptr).
 int helmholtz(lfm_context* ctx, const float* pr, const float* pi, float* sa_raw, int N,
               double gamma, double d, cudaStream_t stream, bool use_ctx_scratch,
-              float** sa_used) {
+              float** sa_used, const float* energy = nullptr) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   FftSlot* s = nullptr;
   int rc = fft_slot(ctx, N, use_ctx_scratch, &s);
   if (rc) return rc;
   float* dst = use_ctx_scratch ? s->sa_raw : sa_raw;
-  cudaError_t e = lfm::launch_color_energy(pr, pi, dst, N, stream);
-  if (e != cudaSuccess) return cuda_fail(e, "|Psi_a|^2 launch");
+  cudaError_t e;
+  const float* src = energy;
+  if (!src) {
+    e = lfm::launch_color_energy(pr, pi, dst, N, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "|Psi_a|^2 launch");
+    src = dst;
+  }
   if (lfm::helmholtz_xpass_supported(N) && g_sa_split.load()) {
     float* table = nullptr;
     rc = split_transform(s, N, gamma, d, stream, &table);
     if (rc) return rc;
     if (cufftSetStream(s->r2c_2d, stream) != CUFFT_SUCCESS ||
-        cufftExecR2C(s->r2c_2d, dst, reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
+        cufftExecR2C(s->r2c_2d, const_cast<float*>(src),
+                     reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
       return fail(LFM_ERR_CUFFT, "cufftExecR2C 2-D N=%d", N);
     e = lfm::launch_helmholtz_xpass(s->spec, table, s->twiddles, N, stream);
     if (e != cudaSuccess) return cuda_fail(e, "Helmholtz pass along i");
@@ -319,7 +327,8 @@ int helmholtz(lfm_context* ctx, const float* pr, const float* pi, float* sa_raw,
     return LFM_OK;
   }
   if (cufftSetStream(s->r2c, stream) != CUFFT_SUCCESS ||
-      cufftExecR2C(s->r2c, dst, reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
+      cufftExecR2C(s->r2c, const_cast<float*>(src),
+                   reinterpret_cast<cufftComplex*>(s->spec)) != CUFFT_SUCCESS)
     return fail(LFM_ERR_CUFFT, "cufftExecR2C N=%d", N);
   e = lfm::launch_helmholtz_multiply_gd(s->spec, N, gamma, d, stream);
   if (e != cudaSuccess) return cuda_fail(e, "Helmholtz multiply launch");
@@ -814,6 +823,20 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
                            double e0_sq, double epsilon_w, double kappa_c, double epsilon_cc,
                            double kappa_string, double kappa_tube, const float* sa,
                            void* stream) {
+  return lfm_leapfrog_color_energy_f32(psi_r, psi_r_prev_io, psi_i, psi_i_prev_io, chi,
+                                       chi_prev_io, mask_table, lut, damp_prev, N, dt2, kappa,
+                                       lambda_self, chi0, e0_sq, epsilon_w, kappa_c, epsilon_cc,
+                                       kappa_string, kappa_tube, sa, nullptr, stream);
+}
+
+int lfm_leapfrog_color_energy_f32(const float* psi_r, float* psi_r_prev_io, const float* psi_i,
+                                  float* psi_i_prev_io, const float* chi, float* chi_prev_io,
+                                  const float* mask_table, const lfm_mask_lut* lut,
+                                  int damp_prev, int N, double dt2, double kappa,
+                                  double lambda_self, double chi0, double e0_sq,
+                                  double epsilon_w, double kappa_c, double epsilon_cc,
+                                  double kappa_string, double kappa_tube, const float* sa,
+                                  float* energy_out, void* stream) {
   int rc = check_n(N);
   if (rc) return rc;
   if (!psi_r || !psi_r_prev_io || !psi_i || !psi_i_prev_io || !chi || !chi_prev_io)
@@ -822,7 +845,8 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
   if (rc) return rc;
   const size_t b = sizeof(float) * (size_t)N * N * N, b3 = 3 * b;
   rc = check_disjoint({{psi_r, b3}, {psi_i, b3}, {chi, b}, {sa, sa ? b3 : 0}},
-                      {{psi_r_prev_io, b3}, {psi_i_prev_io, b3}, {chi_prev_io, b}});
+                      {{psi_r_prev_io, b3}, {psi_i_prev_io, b3}, {chi_prev_io, b},
+                       {energy_out, energy_out ? b3 : 0}});
   if (rc) return rc;
   lfm::StepArgs a{};
   a.level = LFM_COLOR;
@@ -835,6 +859,7 @@ int lfm_leapfrog_color_f32(const float* psi_r, float* psi_r_prev_io, const float
   a.lut = device_lut(mask_table, lut);
   a.damp_prev = damp_prev ? 1 : 0;
   a.sa = (kappa_tube > 0.0) ? sa : nullptr;
+  a.energy_out = energy_out;
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
@@ -965,6 +990,18 @@ int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_
   if (rc) return rc;
   return helmholtz(ctx, psi_r, psi_i, sa_raw, N, sa_gamma, sa_d,
                    static_cast<cudaStream_t>(stream), false, nullptr);
+}
+
+int lfm_helmholtz_sa_from_energy_f32(lfm_context* ctx, const float* energy, float* sa_raw,
+                                     int N, double sa_gamma, double sa_d, void* stream) {
+  int rc = check_n(N);
+  if (rc) return rc;
+  if (!ctx || !energy || !sa_raw) return fail(LFM_ERR_INVALID_ARG, "null argument");
+  const size_t b3 = 3 * sizeof(float) * (size_t)N * N * N;
+  rc = check_disjoint({{energy, b3}}, {{sa_raw, b3}});
+  if (rc) return rc;
+  return helmholtz(ctx, nullptr, nullptr, sa_raw, N, sa_gamma, sa_d,
+                   static_cast<cudaStream_t>(stream), false, nullptr, energy);
 }
 
 int lfm_sa_clip_f32(const float* sa_raw, float* sa_out, int64_t count, void* stream) {

@@ -32,6 +32,7 @@ struct StepArgs {
   MaskLut lut;         // used when mask is null
   const float* sa;     // raw S_a (3*N^3) or null
   float* sa_clip_out;  // clipped S_a copy (protocol colour step) or null
+  float* energy_out;   // COLOR: |Psi_a|^2 of the new fields (3*N^3) or null
   int damp_prev;       // multiply the previous-step fields by (1-mask) on read
   int comp;            // compensated Delta form: *_prev hold increments, updated in place
   // Split chi (REAL, COMPLEX; resident layout only): chi = chi0 + hi + lo with

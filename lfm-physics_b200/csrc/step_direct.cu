@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
             lap19(I), I.c, prev_value(a, a.pi_prev + c * n3, x, absorb), faces_of(I), a.c);
         a.pr_out[c * n3 + x] = o.pr;
         a.pi_out[c * n3 + x] = o.pi;
+        if (a.energy_out) a.energy_out[c * n3 + x] = fadd(fmul(o.pr, o.pr), fmul(o.pi, o.pi));
         if (a.pr_prev_out) a.pr_prev_out[c * n3 + x] = o.pr_prev;
         if (a.pi_prev_out) a.pi_prev_out[c * n3 + x] = o.pi_prev;
       }

@@ -404,6 +404,11 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
       const float o_r[V] = {o.pr.v.x, o.pr.v.y}, o_i[V] = {o.pi.v.x, o.pi.v.y};
       stg<V>(a.pr_out + c * n3 + gofs, o_r);
       stg<V>(a.pi_out + c * n3 + gofs, o_i);
+      if (a.energy_out) {  // |Psi_a|^2 of the stored values, for the next S_a solve
+        const F2 en = fadd(fmul(o.pr, o.pr), fmul(o.pi, o.pi));
+        const float o_e[V] = {en.v.x, en.v.y};
+        stg<V>(a.energy_out + c * n3 + gofs, o_e);
+      }
       if (a.pr_prev_out) {
         const float o_rp[V] = {o.pr_prev.v.x, o.pr_prev.v.y};
         stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
@@ -456,6 +461,12 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
       }
       stg<V>(a.pr_out + c * n3 + gofs, o_r);
       stg<V>(a.pi_out + c * n3 + gofs, o_i);
+      if (a.energy_out) {
+        float o_e[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) o_e[e] = fadd(fmul(o_r[e], o_r[e]), fmul(o_i[e], o_i[e]));
+        stg<V>(a.energy_out + c * n3 + gofs, o_e);
+      }
       if (a.pr_prev_out) stg<V>(a.pr_prev_out + c * n3 + gofs, o_rp);
       if (a.pi_prev_out) stg<V>(a.pi_prev_out + c * n3 + gofs, o_ip);
     }
@@ -1674,7 +1685,7 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   // every copy source and every vector store needs 16-byte alignment
   const void* ptrs[] = {a.pr, a.pi, a.chi, a.pr_prev, a.pi_prev, a.chi_prev, a.pr_out, a.pi_out,
                         a.chi_out, a.pr_prev_out, a.pi_prev_out, a.chi_prev_out, a.mask, a.sa,
-                        a.sa_clip_out, a.chi_lo, a.chi_lo_prev, a.chi_lo_out};
+                        a.sa_clip_out, a.chi_lo, a.chi_lo_prev, a.chi_lo_out, a.energy_out};
   for (const void* p : ptrs)
     if (p && !aligned16(p)) return cudaErrorNotSupported;
 

@@ -73,6 +73,9 @@ _SIGNATURES = {
     "lfm_leapfrog_complex_f32": [_P] * 7 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6 + [_P],
     "lfm_leapfrog_color_f32": [_P] * 7 + [POINTER(MaskLut), c_int, c_int] + [_D] * 10
     + [_P, _P],
+    "lfm_leapfrog_color_energy_f32": [_P] * 7 + [POINTER(MaskLut), c_int, c_int] + [_D] * 10
+    + [_P, _P, _P],
+    "lfm_helmholtz_sa_from_energy_f32": [_P] * 3 + [c_int, _D, _D, _P],
     "lfm_leapfrog_real_comp_f32": [_P] * 7 + [POINTER(MaskLut), c_int] + [_D] * 5 + [_P],
     "lfm_leapfrog_complex_comp_f32": [_P] * 10 + [POINTER(MaskLut), c_int] + [_D] * 6 + [_P],
     "lfm_leapfrog_real_split_f32": [_P] * 7 + [POINTER(MaskLut), c_int, c_int] + [_D] * 5

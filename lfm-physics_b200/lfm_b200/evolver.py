@@ -95,6 +95,11 @@ class Evolver:
             self._cur = 0
             self._damp = False  # prev slots already hold the damped field
             self._sa_raw = torch.zeros(3 * n, **f32) if self._sa_on else None
+            # |Psi_a|^2 of the current fields, written by the previous step's kernel
+            # (valid while nothing else has written Psi since): the next S_a solve
+            # starts from it instead of reading the six Psi arrays again
+            self._energy = torch.empty(3 * n, **f32) if self._sa_on else None
+        self._energy_ok = False
         else:
             self._ab = {
                 "psi_r_A": torch.zeros(psi_n, **f32), "psi_r_prev_A": torch.zeros(psi_n, **f32),
@@ -143,16 +148,22 @@ class Evolver:
             return self._sa_raw
         raise AttributeError(name)
 
+    def _exposed(self, name: str):
+        """A Psi buffer handed to a caller that may write it (the reference's hooks
+        address psi_r_A ... by name): the next step forms |Psi_a|^2 afresh."""
+        self._energy_ok = False
+        return self._buf(name)
+
     # In resident mode the A and B names both refer to the active slots
     # (the inactive set of the reference holds values no step reads).
-    psi_r_A = property(lambda s: s._buf("psi_r_A"))
-    psi_r_B = property(lambda s: s._buf("psi_r_B"))
-    psi_r_prev_A = property(lambda s: s._buf("psi_r_prev_A"))
-    psi_r_prev_B = property(lambda s: s._buf("psi_r_prev_B"))
-    psi_i_A = property(lambda s: s._buf("psi_i_A"))
-    psi_i_B = property(lambda s: s._buf("psi_i_B"))
-    psi_i_prev_A = property(lambda s: s._buf("psi_i_prev_A"))
-    psi_i_prev_B = property(lambda s: s._buf("psi_i_prev_B"))
+    psi_r_A = property(lambda s: s._exposed("psi_r_A"))
+    psi_r_B = property(lambda s: s._exposed("psi_r_B"))
+    psi_r_prev_A = property(lambda s: s._exposed("psi_r_prev_A"))
+    psi_r_prev_B = property(lambda s: s._exposed("psi_r_prev_B"))
+    psi_i_A = property(lambda s: s._exposed("psi_i_A"))
+    psi_i_B = property(lambda s: s._exposed("psi_i_B"))
+    psi_i_prev_A = property(lambda s: s._exposed("psi_i_prev_A"))
+    psi_i_prev_B = property(lambda s: s._exposed("psi_i_prev_B"))
     chi_A = property(lambda s: s._buf("chi_A"))
     chi_B = property(lambda s: s._buf("chi_B"))
     chi_prev_A = property(lambda s: s._buf("chi_prev_A"))
@@ -170,6 +181,7 @@ class Evolver:
     def native_psi_real(self):
         """The current Psi_r buffer as an (N, N, N) device view ((3, N, N, N) at COLOR):
         edits are seen by the next step.  The previous-step buffers are not exposed."""
+        self._energy_ok = False  # the caller may edit Psi through the view
         if self._mode == "ab":
             return self._view(self._ab["psi_r_A" if self._use_buffer_A else "psi_r_B"])
         return self._view(self._pr[self._cur])
@@ -178,6 +190,7 @@ class Evolver:
         """The current Psi_i buffer as a device view, None at the REAL level."""
         if not self._has_imag:
             return None
+        self._energy_ok = False
         if self._mode == "ab":
             return self._view(self._ab["psi_i_A" if self._use_buffer_A else "psi_i_B"])
         return self._view(self._pi[self._cur])
@@ -283,7 +296,7 @@ class Evolver:
         if g is None:
             for h in hooks:
                 h.prepare_block(self, K)
-            saved = (self._cur, self._damp, self._use_buffer_A)
+            saved = (self._cur, self._damp, self._use_buffer_A, self._energy_ok)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 for k in range(K):
@@ -291,7 +304,7 @@ class Evolver:
                     self._use_buffer_A = not self._use_buffer_A
                     for h in hooks:
                         h.apply_in_block(self, k)
-            self._cur, self._damp, self._use_buffer_A = saved
+            self._cur, self._damp, self._use_buffer_A, self._energy_ok = saved
             self._hgraphs[key] = (g, list(hooks))  # the graph holds the hooks' buffers
         return self._hgraphs[key][0]
 
@@ -310,19 +323,19 @@ class Evolver:
         key = self._param_key()
         g = self._graphs.get(key)
         if g is None:
-            saved = (self._cur, self._damp, self._use_buffer_A)
+            saved = (self._cur, self._damp, self._use_buffer_A, self._energy_ok)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 self._step_resident()
                 self._step_resident()
-            self._cur, self._damp, self._use_buffer_A = saved
+            self._cur, self._damp, self._use_buffer_A, self._energy_ok = saved
             self._graphs[key] = g
         return g
 
     def warm_graphs(self) -> None:
         """Capture the two-step graphs of both slot parities now (nothing runs), so a
         later evolve() does not capture inside a timed region.  Needs one step done."""
-        if self._mode != "resident" or not self._damp:
+        if self._mode != "resident" or not self._damp or (self._sa_on and not self._energy_ok):
             return
         saved = self._cur
         for c in (0, 1):
@@ -333,8 +346,9 @@ class Evolver:
     def _evolve_graphed(self, steps: int) -> None:
         self._dt2 = self.config.dt**2
         done = 0
-        if not self._damp:
-            # first step after a host write: the kernel must not damp prev
+        if not self._damp or (self._sa_on and not self._energy_ok):
+            # first step after a host write: the kernel must not damp prev, and
+            # |Psi_a|^2 comes from Psi, not from the previous step's kernel
             self._step()
             self.step += 1
             done = 1
@@ -374,19 +388,26 @@ class Evolver:
                       self._chi[cur].data_ptr(), self._chi[prv].data_ptr(), table, desc, damp,
                       self.N, *common, float(cfg.epsilon_w), stream)
         else:
-            sa = None
+            sa = energy = None
             if self._sa_on:
-                _lib.call("lfm_helmholtz_sa_f32", self.backend.context.handle,
-                          self._pr[cur].data_ptr(), self._pi[cur].data_ptr(),
-                          self._sa_raw.data_ptr(), self.N, float(cfg.sa_gamma), float(cfg.sa_d),
-                          stream)
+                ctx = self.backend.context.handle
+                if self._energy_ok:
+                    _lib.call("lfm_helmholtz_sa_from_energy_f32", ctx, self._energy.data_ptr(),
+                              self._sa_raw.data_ptr(), self.N, float(cfg.sa_gamma),
+                              float(cfg.sa_d), stream)
+                else:
+                    _lib.call("lfm_helmholtz_sa_f32", ctx, self._pr[cur].data_ptr(),
+                              self._pi[cur].data_ptr(), self._sa_raw.data_ptr(), self.N,
+                              float(cfg.sa_gamma), float(cfg.sa_d), stream)
                 sa = self._sa_raw.data_ptr()
-            _lib.call("lfm_leapfrog_color_f32", self._pr[cur].data_ptr(), self._pr[prv].data_ptr(),
-                      self._pi[cur].data_ptr(), self._pi[prv].data_ptr(),
-                      self._chi[cur].data_ptr(), self._chi[prv].data_ptr(), table, desc, damp,
-                      self.N, *common, float(cfg.epsilon_w), float(cfg.kappa_c),
-                      float(cfg.epsilon_cc), float(cfg.kappa_string), float(cfg.kappa_tube), sa,
-                      stream)
+                energy = self._energy.data_ptr()
+            _lib.call("lfm_leapfrog_color_energy_f32", self._pr[cur].data_ptr(),
+                      self._pr[prv].data_ptr(), self._pi[cur].data_ptr(),
+                      self._pi[prv].data_ptr(), self._chi[cur].data_ptr(),
+                      self._chi[prv].data_ptr(), table, desc, damp, self.N, *common,
+                      float(cfg.epsilon_w), float(cfg.kappa_c), float(cfg.epsilon_cc),
+                      float(cfg.kappa_string), float(cfg.kappa_tube), sa, energy, stream)
+            self._energy_ok = self._sa_on
         self._cur = prv
         self._damp = True
 
@@ -424,7 +445,7 @@ class Evolver:
     # ------------------------------------------------------------------
     def _active(self, field: str):
         s = "A" if self._use_buffer_A else "B"
-        return getattr(self, f"{field}_{s}")
+        return self._buf(f"{field}_{s}")
 
     def _prev_psi_view(self, imag: bool):
         """Previous Psi with the sponge factor applied, as the reference stores it."""
@@ -560,6 +581,7 @@ class Evolver:
     def _write(self, names, data) -> None:
         """Copy `data` (host or device) into the named buffers: one host->device
         copy (asynchronous from pinned memory), device->device for the rest."""
+        self._energy_ok = False
         first = None
         seen = set()
         for nm in names:
@@ -593,11 +615,13 @@ class Evolver:
         self._write(("psi_i_prev_A", "psi_i_prev_B"), self._dev(arr))
 
     def set_psi_real_current(self, arr) -> None:
+        self._energy_ok = False
         self._active("psi_r").copy_(self._dev(arr), non_blocking=True)
 
     def set_psi_imag_current(self, arr) -> None:
         if not self._has_imag:
             raise ValueError("Cannot set imaginary part for REAL field level")
+        self._energy_ok = False
         self._active("psi_i").copy_(self._dev(arr), non_blocking=True)
 
     def set_chi(self, arr) -> None:

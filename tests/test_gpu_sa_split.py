@@ -112,3 +112,58 @@ def test_color_evolver_64_with_split_transform_against_oracle(be):
                       (ev.get_chi().ravel(), lat.chi)):
         err = np.abs(got.astype(np.float64) - want).max() / np.abs(want).max()
         assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("N", [32, 64])
+def test_energy_from_the_step_epilogue_equals_a_fresh_energy_pass(be, N):
+    """A step writes |Psi_a|^2 of its new fields and the next S_a solve starts from it
+    (lfm_leapfrog_color_energy_f32 + lfm_helmholtz_sa_from_energy_f32): the same bits as
+    forming |Psi_a|^2 from Psi before every solve (the separate energy pass)."""
+    from lfm_b200 import Evolver
+    from lfm_b200.config import full_physics
+
+    cfg = full_physics(N)
+    pr, pi = _packets(N, 11)
+    runs = []
+    for reuse in (True, False):
+        ev = Evolver(cfg, backend=be)
+        ev.set_psi_real(pr.reshape(3, N, N, N))
+        ev.set_psi_imag(pi.reshape(3, N, N, N))
+        if reuse:
+            ev.evolve(13)  # graphs of two steps, energy handed from step to step
+        else:
+            ev.use_graphs = False
+            for _ in range(13):
+                ev._energy_ok = False  # form |Psi_a|^2 from Psi before each solve
+                ev.evolve(1)
+        runs.append((ev.get_psi_real(), ev.get_psi_imag(), ev.get_chi(), ev.get_sa_fields()))
+    for a, b in zip(*runs):
+        assert np.array_equal(np.ascontiguousarray(a).view(np.uint32),
+                              np.ascontiguousarray(b).view(np.uint32))
+
+
+def test_psi_writes_invalidate_the_handed_energy(be):
+    """After set_psi_real / set_psi_imag_current between steps, the next solve forms
+    |Psi_a|^2 from the new Psi (the oracle agrees within the COLOR tolerance)."""
+    from lfm_b200 import Evolver
+    from lfm_b200.config import full_physics
+
+    N = 32
+    cfg = full_physics(N)
+    pr, pi = _packets(N, 12)
+    ev = Evolver(cfg, backend=be)
+    ev.set_psi_real(pr.reshape(3, N, N, N))
+    ev.set_psi_imag(pi.reshape(3, N, N, N))
+    ev.evolve(6)
+    new_i = (1.1 * ev.get_psi_imag()).astype(np.float32)
+    ev.set_psi_imag_current(new_i)
+    ev.evolve(6)
+    lat = O.OracleLattice(cfg)
+    lat.set_psi_real(pr)
+    lat.set_psi_imag(pi)
+    lat.step(6)
+    lat.pi[:] = new_i.ravel()
+    lat.step(6)
+    for got, want in ((ev.get_psi_real().ravel(), lat.pr), (ev.get_chi().ravel(), lat.chi)):
+        err = np.abs(got.astype(np.float64) - want).max() / np.abs(want).max()
+        assert err < 1e-5, err
