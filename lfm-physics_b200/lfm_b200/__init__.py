@@ -25,6 +25,7 @@ __all__ = [
     "gravity_only",
     "B200Backend",
     "Evolver",
+    "SplitChiEvolver",
     "get_backend",
 ]
 
@@ -39,4 +40,8 @@ def __getattr__(name):
         from .evolver import Evolver
 
         return Evolver
+    if name == "SplitChiEvolver":
+        from .split import SplitChiEvolver
+
+        return SplitChiEvolver
     raise AttributeError(name)
