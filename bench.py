@@ -479,15 +479,17 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
     cfg = gravity_em(N)
     (amp, cen, ph), pert, sigma = adjoint_packets(N)
     params = [t.to(dev).float() for t in (amp, cen, ph)]
+    od = cfg.chi0 * cfg.dt  # packets rotating as Simulation.place_soliton starts them
     with torch.no_grad():
-        st = soliton_state(N, *[t.to(dev).float() for t in pert], sigma, cfg.chi0, None, True)
+        st = soliton_state(N, *[t.to(dev).float() for t in pert], sigma, cfg.chi0, None, True,
+                           omega_dt=od)
         target = leapfrog(cfg, st, steps, backend=be)[4].clone()
     stream = torch.cuda.current_stream(dev)
 
     def one(timed: bool):
         p = [t.clone().requires_grad_(True) for t in params]
         dchi = torch.zeros((N, N, N), device=dev, requires_grad=True)
-        st = soliton_state(N, *p, sigma, cfg.chi0, dchi, True)
+        st = soliton_state(N, *p, sigma, cfg.chi0, dchi, True, omega_dt=od)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         torch.cuda.synchronize(dev)
         barrier()

@@ -309,19 +309,25 @@ def memory_bytes(config, steps: int, every: int | None = None) -> dict:
 
 # ------------------------------------------------------------------ initial states
 def soliton_state(N: int, amplitude, centre, phase, sigma: float, chi0: float, dchi=None,
-                  complex_level: bool = True, device=None, dtype=torch.float32):
+                  complex_level: bool = True, device=None, dtype=torch.float32,
+                  omega_dt: float | None = None):
     """Differentiable initial state: a sum of Gaussian packets.
 
     amplitude (S,), centre (S, 3), phase (S,) tensors; packet s is
     amplitude_s exp(-|x - centre_s|^2 / (2 sigma^2)) e^{i phase_s} (as
     lfm/fields/soliton.py:49-59 builds them, without wrap).  chi = chi0 +
-    dchi.  Previous fields equal the current ones, as set_psi_real /
-    set_chi leave them.  Returns the six state tensors.
+    dchi.  Without omega_dt the previous fields equal the current ones, as
+    set_psi_real / set_chi leave them; with omega_dt (COMPLEX) each packet's
+    previous value carries the phase phase_s + omega_dt, the rotation of a
+    packet at rest that the reference's Simulation.place_soliton gives it
+    (lfm/simulation.py:585-591, omega = chi0 for zero momentum).  Returns the
+    six state tensors.
     """
     dev = device if device is not None else amplitude.device
     x = torch.arange(N, device=dev, dtype=dtype)
     pr = torch.zeros((N, N, N), device=dev, dtype=dtype)
     pi = torch.zeros((N, N, N), device=dev, dtype=dtype)
+    prp, pip = pr, pi
     for s in range(amplitude.shape[0]):
         c = centre[s].to(dtype)
         d2 = ((x - c[0]) ** 2)[:, None, None] + ((x - c[1]) ** 2)[None, :, None] \
@@ -330,9 +336,14 @@ def soliton_state(N: int, amplitude, centre, phase, sigma: float, chi0: float, d
         th = phase[s].to(dtype)
         pr = pr + env * torch.cos(th)
         pi = pi + env * torch.sin(th)
+        if omega_dt is not None:
+            prp = prp + env * torch.cos(th + omega_dt)
+            pip = pip + env * torch.sin(th + omega_dt)
     chi = torch.full((N, N, N), float(chi0), device=dev, dtype=dtype)
     if dchi is not None:
         chi = chi + dchi.to(dtype)
+    if omega_dt is None:
+        prp, pip = pr, pi
     if complex_level:
-        return [pr, pr, pi, pi, chi, chi]
-    return [pr, pr, None, None, chi, chi]
+        return [pr, prp, pi, pip, chi, chi]
+    return [pr, prp, None, None, chi, chi]

@@ -85,6 +85,7 @@ class Evolver:
         else:
             self._absorb_psi = self._absorb
 
+        self._energy_ok = False
         if self._mode == "resident":
             self._table_dev = self._table.to_device(self.device)
             self._desc = self._table.desc
@@ -99,7 +100,6 @@ class Evolver:
             # (valid while nothing else has written Psi since): the next S_a solve
             # starts from it instead of reading the six Psi arrays again
             self._energy = torch.empty(3 * n, **f32) if self._sa_on else None
-        self._energy_ok = False
         else:
             self._ab = {
                 "psi_r_A": torch.zeros(psi_n, **f32), "psi_r_prev_A": torch.zeros(psi_n, **f32),

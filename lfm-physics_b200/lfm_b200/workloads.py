@@ -133,9 +133,12 @@ def adjoint_packets(N: int = 96, seed: int = 6):
     amplitudes U[4, 6] and phases U[0, 2 pi) (seed).  The target run uses
     different parameters drawn from the same generator: amplitudes x U[1.15,
     1.35], centres moved by U[-2, 2] cells per axis, phases moved by U[-0.8,
-    0.8].  chi's deviation from chi0 then differs between the two runs by a
-    sizeable fraction of itself, so the loss |chi_T - chi_target|^2 and its
-    gradients stand well above float32 rounding.
+    0.8].  The runs start the packets rotating as the reference's
+    Simulation.place_soliton does (previous phase + chi0 dt; soliton_state's
+    omega_dt), so |Psi|^2 stays put while chi responds.  Under gravity_em at
+    dt = 0.02, chi's forced oscillation is near the end of a cycle at step 500:
+    chi_T lies within ~1e-5 of chi0, and the two runs' chi differ by ~3e-5
+    there, against ~1e-3 mid-run.
 
     Returns ((amplitude (2,), centre (2, 3), phase (2,)), (the target's three),
     sigma), float64 torch tensors on the CPU.

@@ -227,3 +227,19 @@ def test_product_does_not_import_the_oracle():
     for p in list(pkg.rglob("*.py")) + list(pkg.rglob("*.cu")) + list(pkg.rglob("*.cuh")):
         text = p.read_text()
         assert not re.search(r"(from|import)\s+oracle|lfm_oracle|oracle/", text), p
+
+
+def test_every_python_source_compiles():
+    """Every module of the package, the tests, the oracle and bench.py byte-compile (a
+    syntax error in a GPU-only module would otherwise surface only on the GPU machine)."""
+    import py_compile
+    import tempfile
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    files = [root / "bench.py", root / "__graft_entry__.py"]
+    for d in ("lfm-physics_b200/lfm_b200", "tests", "tests/golden", "oracle"):
+        files += sorted((root / d).glob("*.py"))
+    with tempfile.TemporaryDirectory() as tmp:
+        for i, f in enumerate(files):
+            py_compile.compile(str(f), cfile=str(Path(tmp) / f"{i}.pyc"), doraise=True)
