@@ -63,6 +63,8 @@ def parse():
                     help="approximate CPU time of the oracle baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-main", action="store_true",
+                    help="skip the main leg (profiling runs of the other legs; no main value)")
     ap.add_argument("--no-compensated", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the split-chi leg")
     ap.add_argument("--no-batched", action="store_true")
@@ -564,14 +566,15 @@ def run_b200(args):
         main_cfg = gravity_em(N)
     else:
         main_cfg = gravity_only(N)
-    ev = Evolver(main_cfg, backend=be)
-    ev.set_psi_real(E)
-    if complex_level:
-        ev.set_psi_imag(0.5 * E)
-    ev.set_chi(chi)
-    ev.evolve(max(args.warmup, 3))
-    ev.warm_graphs()
-    torch.cuda.synchronize(dev)
+    if not args.no_main:
+        ev = Evolver(main_cfg, backend=be)
+        ev.set_psi_real(E)
+        if complex_level:
+            ev.set_psi_imag(0.5 * E)
+        ev.set_chi(chi)
+        ev.evolve(max(args.warmup, 3))
+        ev.warm_graphs()
+        torch.cuda.synchronize(dev)
 
     def barrier():
         if world > 1:
@@ -593,7 +596,8 @@ def run_b200(args):
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
-    ev.evolve(args.steps)
+    if not args.no_main:
+        ev.evolve(args.steps)
     t_end.record(stream)
     torch.cuda.synchronize(dev)
     barrier()
@@ -603,6 +607,8 @@ def run_b200(args):
     if status:
         raise RuntimeError(f"device status word {status} after the timed steps")
     cells = N**3
+    if args.no_main:  # profiling runs of the other legs only: no main figure
+        ms = float("nan")
     value = world * cells * args.steps / (ms / 1e3) / 1e9
     ms_per_step = ms / args.steps
     cfg_used = _lib.tune_get(int(main_cfg.field_level), N)
