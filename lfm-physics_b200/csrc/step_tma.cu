@@ -1482,37 +1482,37 @@ std::mutex FixedSlot<LEVEL, V, N, TJ, S, MODE>::mu;
 template <int LEVEL, int V, int N, int TJ, int S, int MODE>
 int FixedSlot<LEVEL, V, N, TJ, S, MODE>::granted = 0;
 
+// The compile-time tiles: step form, level, cells per lane, N, rows, stages.
+// The compensated step has one at the throughput size; split chi at REAL 256^3
+// and 512^3 (its ring is COMPLEX-shaped: three stencil and three point fields).
 struct FixedTile {
-  int level, V, N, TJ, S;
+  int mode, level, V, N, TJ, S;
 };
 constexpr FixedTile kFixedTiles[] = {
-    {LFM_REAL, 4, 512, 4, 3}, {LFM_REAL, 4, 256, 8, 3}, {LFM_COMPLEX, 2, 512, 2, 3},
-    {LFM_COMPLEX, 2, 256, 4, 3}, {LFM_REAL, 4, 128, 8, 3}, {LFM_COMPLEX, 2, 128, 4, 3}};
+    {kPlain, LFM_REAL, 4, 512, 4, 3},    {kPlain, LFM_REAL, 4, 256, 8, 3},
+    {kPlain, LFM_COMPLEX, 2, 512, 2, 3}, {kPlain, LFM_COMPLEX, 2, 256, 4, 3},
+    {kPlain, LFM_REAL, 4, 128, 8, 3},    {kPlain, LFM_COMPLEX, 2, 128, 4, 3},
+    {kComp, LFM_REAL, 4, 512, 4, 3},     {kSplit, LFM_REAL, 2, 512, 2, 3},
+    {kSplit, LFM_REAL, 2, 256, 4, 3}};
 
-// The stage count of the compile-time tile (level, V, N, TJ); 0 if none.
-constexpr int fixed_stages(int level, int V, int N, int TJ) {
+// The stage count of the compile-time tile (mode, level, V, N, TJ); 0 if none.
+constexpr int fixed_stages(int mode, int level, int V, int N, int TJ) {
   for (const FixedTile& t : kFixedTiles)
-    if (t.level == level && t.V == V && t.N == N && t.TJ == TJ) return t.S;
+    if (t.mode == mode && t.level == level && t.V == V && t.N == N && t.TJ == TJ) return t.S;
   return 0;
 }
 
-// The fixed tile for (level, V, N), if any.
-const FixedTile* fixed_tile(int level, int V, int N) {
+// The fixed tile for (mode, level, V, N), if any.
+const FixedTile* fixed_tile(int mode, int level, int V, int N) {
   for (const FixedTile& t : kFixedTiles)
-    if (t.level == level && t.V == V && t.N == N) return &t;
+    if (t.mode == mode && t.level == level && t.V == V && t.N == N) return &t;
   return nullptr;
 }
 
 template <int LEVEL, int V, int N, int TJ, int MODE = kPlain>
 cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(LEVEL, V, N, TJ), MODE>;
+  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(MODE, LEVEL, V, N, TJ), MODE>;
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
-}
-
-// Which step forms have compile-time tiles: the plain step at every size of
-// kFixedTiles, the compensated step at the throughput size only, split chi none.
-constexpr bool has_fixed(int mode, int level, int N) {
-  return mode == kPlain || (mode == kComp && level == LFM_REAL && N == 512);
 }
 
 // Shared memory of the sponge table of the compile-time tiles: count entries
@@ -1526,12 +1526,15 @@ int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
 template <int LEVEL, int V, int MODE = kPlain>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
   if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
-  if (!has_fixed(MODE, LEVEL, P.N)) return false;
-  const FixedTile* t = fixed_tile(LEVEL, V, P.N);
+  const FixedTile* t = fixed_tile(MODE, LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
   if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
     return false;
   if constexpr (MODE == kSplit) {
+    if constexpr (LEVEL == LFM_REAL && V == 2) {
+      if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 2, kSplit>(P, ch, stream); return true; }
+      if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 4, kSplit>(P, ch, stream); return true; }
+    }
     return false;
   } else if constexpr (MODE == kComp) {
     if constexpr (LEVEL == LFM_REAL && V == 4) {
@@ -1570,9 +1573,8 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
   // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
-  const FixedTile* ft = (QUEUE && has_fixed(MODE, LEVEL, P.N) && P.pf_mask < 0 &&
-                         P.pf_sa < 0 && P.np == P.ns && !P.a.slab)
-                            ? fixed_tile(LEVEL, V, P.N) : nullptr;
+  const FixedTile* ft = (QUEUE && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns && !P.a.slab)
+                            ? fixed_tile(MODE, LEVEL, V, P.N) : nullptr;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {
     fixed_cfg = TileConfig{ft->TJ, ft->S, 0, 0, 0, V};
