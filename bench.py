@@ -407,9 +407,11 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
 def run_color(args, be, dev, world, barrier, max_over_ranks, peak):
     """COLOR step (full_physics, three complex colours, S_a solved every step) on two
     colour-charged packets 40 cells apart with chi = 19 +- 1e-3, device-timed over
-    `color_steps` graph-replayed steps on every rank (its own lattice each).  The fused stencil kernel moves 84 B/cell
-    (Psi_a, chi and their previous values in, new values out) plus 12 B/cell of S_a;
-    the S_a solve adds |Psi_a|^2, three R2C/C2R cuFFT pairs and the k-space filter.
+    `color_steps` graph-replayed steps on every rank (its own lattice each).  The fused
+    stencil kernel moves 84 B/cell (Psi_a, chi and their previous values in, new values
+    out) plus 12 B/cell of S_a read and 12 B/cell of |Psi_a|^2 written for the next
+    solve; the S_a solve is a 2-D R2C over (j, k), the fused pass along i (FFT, filter,
+    inverse FFT) and a 2-D C2R for power-of-two N.
     The same lattice without the tube coupling (kappa_tube = 0, no S_a) is timed
     beside it to split the step."""
     import torch

@@ -277,6 +277,7 @@ int split_transform(FftSlot* s, int N, double gamma, double d, cudaStream_t stre
     e = cudaMalloc(&s->twiddles, sizeof(float2) * N);
     if (e == cudaSuccess)
       e = cudaMemcpy(s->twiddles, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = lfm::upload_dft_twiddles();  // this context's device
     if (e != cudaSuccess) return cuda_fail(e, "twiddle table");
   }
   float* t = nullptr;

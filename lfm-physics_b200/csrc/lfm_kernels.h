@@ -74,6 +74,9 @@ cudaError_t launch_helmholtz_table(float* table, int N, double gamma, double d,
                                    cudaStream_t stream);
 cudaError_t launch_helmholtz_xpass(float2* spec, const float* table, const float2* twiddles,
                                    int N, cudaStream_t stream);
+// Uploads the register DFTs' twiddles to the current device's constant memory
+// (once per device, before the first pass along i; synchronous).
+cudaError_t upload_dft_twiddles();
 
 // Poisson equilibration pieces (poisson.cu).
 cudaError_t launch_poisson_rhs(const float* pr, const float* pi, float* rhs, int N, int colours,

@@ -20,7 +20,9 @@
 // registers; the inverse retraces the steps with conjugate twiddles, so every
 // thread ends with the elements it loaded.  The register DFTs are iterative
 // radix-2 Cooley-Tukey (decimation in time).  Twiddles w_N^j = e^{-2 pi i j/N}
-// come from a table computed on the host in double precision.
+// come from tables computed on the host in double precision: the length-N
+// table in shared memory for the twiddles between the two DFTs, and the
+// length-32 table in constant memory for the register DFTs (M <= 32).
 //
 // The filter factor of each spectral point, gamma/(gamma + D k^2) / N^3
 // rounded to float32 once, is read from a table over (|fx|, |fy|, fz) built by
@@ -28,6 +30,8 @@
 // (k = 2 pi fftfreq(N)); k^2 depends only on the magnitudes of the integer
 // frequencies, so (N/2+1)^3 entries cover the spectrum.
 #include "lfm_kernels.h"
+
+#include <cmath>
 
 namespace lfm {
 namespace {
@@ -45,10 +49,18 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
 
+// e^{-2 pi i t / 32}, t < 32: the twiddles of the register DFTs (M <= 32),
+// w_M^u = c_w32[u * 32 / M].  The indices are compile-time constants, so each
+// twiddle is an operand from the constant bank, not a shared-memory load.
+// The values equal the pass's own table (e^{-2 pi i (u N / M) / N} has the same
+// angle u / M in double).
+__constant__ float2 c_w32[32];
+
 // One radix-2 stage (butterflies of span LEN / 2) of an in-register DFT of
 // size M; a[] is in bit-reversed order before the first stage.
 template <int M, int LEN, bool INV>
-__device__ __forceinline__ void dft_stage(float2 (&a)[M], const float2* tw, int stride) {
+__device__ __forceinline__ void dft_stage(float2 (&a)[M]) {
+  static_assert(M <= 32, "register DFTs take their twiddles from c_w32");
   constexpr int half = LEN / 2, step = M / LEN;
 #pragma unroll
   for (int i = 0; i < M; i += LEN) {
@@ -60,7 +72,7 @@ __device__ __forceinline__ void dft_stage(float2 (&a)[M], const float2* tw, int 
       } else if (4 * u == M) {  // w_M^(M/4) = -i (forward), +i (inverse)
         t = INV ? make_float2(-t.y, t.x) : make_float2(t.y, -t.x);
       } else {
-        const float2 w = tw[u * stride];
+        const float2 w = c_w32[u * (32 / M)];
         t = cmul(t, INV ? conjf2(w) : w);
       }
       const float2 s = a[i + j];
@@ -68,18 +80,18 @@ __device__ __forceinline__ void dft_stage(float2 (&a)[M], const float2* tw, int 
       a[i + j + half] = make_float2(s.x - t.x, s.y - t.y);
     }
   }
-  if constexpr (LEN < M) dft_stage<M, 2 * LEN, INV>(a, tw, stride);
+  if constexpr (LEN < M) dft_stage<M, 2 * LEN, INV>(a);
 }
 
 // v[k] <- sum_j v[j] w_M^(s j k), s = -1 (forward, e^{-}) or +1 (inverse), in
-// registers.  tw[t] = e^{-2 pi i t / N}; w_M^u = tw[u * N / M].
+// registers.
 template <int M, bool INV>
-__device__ __forceinline__ void dft_reg(float2 (&v)[M], const float2* tw, int N) {
+__device__ __forceinline__ void dft_reg(float2 (&v)[M]) {
   constexpr int B = log2i(M);
   float2 a[M];
 #pragma unroll
   for (int i = 0; i < M; ++i) a[bitrev(i, B)] = v[i];
-  dft_stage<M, 2, INV>(a, tw, N / M);
+  dft_stage<M, 2, INV>(a);
 #pragma unroll
   for (int i = 0; i < M; ++i) v[i] = a[i];
 }
@@ -116,7 +128,7 @@ __global__ void __launch_bounds__(N1* TW) helmholtz_xpass_kernel(float2* __restr
   float2 v[N2];
 #pragma unroll
   for (int m = 0; m < N2; ++m) v[m] = col[(int64_t)(n1 + N1 * m) * W];
-  dft_reg<N2, false>(v, tw, N);  // v[k2] = Y[n1][k2]
+  dft_reg<N2, false>(v);  // v[k2] = Y[n1][k2]
 #pragma unroll
   for (int k2 = 1; k2 < N2; ++k2) v[k2] = cmul(v[k2], tw[n1 * k2]);
 #pragma unroll
@@ -128,7 +140,7 @@ __global__ void __launch_bounds__(N1* TW) helmholtz_xpass_kernel(float2* __restr
     const int k2 = n1 + N1 * g;
 #pragma unroll
     for (int j = 0; j < N1; ++j) u[g][j] = S[(k2 * N1 + j) * TW + c];
-    dft_reg<N1, false>(u[g], tw, N);  // u[g][k1] = X[k2 + N2 k1]
+    dft_reg<N1, false>(u[g]);  // u[g][k1] = X[k2 + N2 k1]
     // ---- the filter --------------------------------------------------------
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
@@ -138,7 +150,7 @@ __global__ void __launch_bounds__(N1* TW) helmholtz_xpass_kernel(float2* __restr
       u[g][k1] = make_float2(u[g][k1].x * f, u[g][k1].y * f);
     }
     // ---- inverse along x, first half ---------------------------------------
-    dft_reg<N1, true>(u[g], tw, N);  // u[g][j] = sum_k1 X w_N1^(-k1 j)
+    dft_reg<N1, true>(u[g]);  // u[g][j] = sum_k1 X w_N1^(-k1 j)
 #pragma unroll
     for (int j = 1; j < N1; ++j) u[g][j] = cmul(u[g][j], conjf2(tw[k2 * j]));
   }
@@ -152,7 +164,7 @@ __global__ void __launch_bounds__(N1* TW) helmholtz_xpass_kernel(float2* __restr
   __syncthreads();
 #pragma unroll
   for (int k2 = 0; k2 < N2; ++k2) v[k2] = S[(k2 * N1 + n1) * TW + c];
-  dft_reg<N2, true>(v, tw, N);  // v[m] = x[n1 + N1 m] (times N: unnormalised)
+  dft_reg<N2, true>(v);  // v[m] = x[n1 + N1 m] (times N: unnormalised)
 #pragma unroll
   for (int m = 0; m < N2; ++m) col[(int64_t)(n1 + N1 * m) * W] = v[m];
 }
@@ -201,6 +213,15 @@ cudaError_t launch_xpass(float2* spec, const float* table, const float2* tw,
 }
 
 }  // namespace
+
+cudaError_t upload_dft_twiddles() {
+  float2 w[32];
+  for (int t = 0; t < 32; ++t) {
+    const double ang = -2.0 * 3.14159265358979323846 * (double)t / 32.0;
+    w[t] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+  }
+  return cudaMemcpyToSymbol(c_w32, w, sizeof(w));
+}
 
 bool helmholtz_xpass_supported(int N) {
   return N == 64 || N == 128 || N == 256 || N == 512 || N == 1024;

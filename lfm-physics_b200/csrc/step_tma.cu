@@ -1372,7 +1372,14 @@ Choice choose(int level, int N, int V, int ns, int np, bool queue, int max_threa
       const int l1_kb = 256 - carveout_kb(ctas * (smem + 1024));
       // (measured at 512^3: a 60-92 KB L1 beside the 67 KB table runs 10-15% slower)
       const bool table_fits = l1_table_bytes == 0 || l1_kb * 1024 >= l1_table_bytes + 48 * 1024;
-      const double score = warps / 48.0 + 0.6 * halo + 0.25 * depth + (table_fits ? 0.5 : 0.0);
+      // The barrier kernel (COLOR) waits for the whole CTA once per plane; a
+      // second CTA on the SM computes meanwhile.  Measured at COLOR 256^3 with
+      // S_a: 2 rows x 4 stages, two 256-thread CTAs per SM, 1.082 ms per step
+      // against 1.112 for 4 rows x 5 stages (one 512-thread CTA); at 128^3
+      // and 64^3 the two shapes were within noise.
+      const double overlap = (!queue && ctas >= 2) ? 0.3 : 0.0;
+      const double score =
+          warps / 48.0 + 0.6 * halo + 0.25 * depth + (table_fits ? 0.5 : 0.0) + overlap;
       if (score > best_score) {
         best_score = score;
         best.TJ = TJ;
