@@ -153,11 +153,12 @@ def test_largest_tested_lattice_fused_and_direct_agree(be):
     assert _lib.device_status() == 0
 
 
-@pytest.mark.parametrize("N", [64, 128])
+@pytest.mark.parametrize("N", [64, 128, 256])
 def test_color_fused_default_tile_bit_exact(be, N):
-    """The COLOR kernel on the planner's own tiles at larger N (4-row tiles, deep
-    rings, point fields from global memory, packed cell math): a few resident steps
-    with every coupling but S_a against the oracle, then one protocol step."""
+    """The COLOR kernel on the planner's own tiles at larger N (two resident CTAs per
+    SM where they fit, point fields from global memory, packed cell math): a few
+    resident steps with every coupling but S_a against the oracle.  At 256^3 the
+    tile is 2 rows x 4 stages, 256 threads."""
     from lfm_b200 import Evolver, _lib
 
     cfg = _parity_config("color", sa=False, N=N)
@@ -178,6 +179,8 @@ def test_color_fused_default_tile_bit_exact(be, N):
         lat.step(3)
         used = _lib.tune_get(2, N)
         assert used["vec"] == 2 and used["tj"] >= 2, used
+        if N == 256:
+            assert (used["tj"], used["stages"], used["threads"]) == (2, 4, 256), used
         assert bits_equal(ev.get_psi_real().ravel(), lat.pr)
         assert bits_equal(ev.get_psi_imag().ravel(), lat.pi)
         assert bits_equal(ev.get_chi().ravel(), lat.chi)
