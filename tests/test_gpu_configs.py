@@ -392,7 +392,7 @@ def test_config5_adjoint_complex96_500_steps(be):
         "N": N, "steps": steps, "workload": "COMPLEX 96^3 gravity_em, two rotating packets "
         "(prev phase + chi0 dt, as Simulation.place_soliton) + per-cell chi offset, loss "
         "|chi_T - chi_target|^2 (lfm_b200.workloads.adjoint_packets)",
-        "loss_f32": float(loss32), "loss_f64": float(loss64),
+        "loss_f32": float(loss32.detach()), "loss_f64": float(loss64.detach()),
         "chi_f32_max_abs_error": float((chi32.detach().double() - chi64).abs().max()),
         "chi_minus_target_max_abs": float((chi64 - target).abs().max()),
         "chi_minus_chi0_max_abs": float((chi64 - cfg.chi0).abs().max()),
