@@ -1150,8 +1150,9 @@ namespace {
 // and COMPLEX items together) and the launch shape.  Pure host arithmetic
 // (lfm_batch_plan exposes it without a device).
 struct BatchPlan {
-  std::vector<lfm::BatchItem> items;  // REAL items, then COMPLEX, each largest first
+  std::vector<lfm::BatchItem> items;  // by shape class (REAL ones first), each largest first
   int real_items = 0;
+  int class_off[lfm::kBatchClasses] = {}, class_n[lfm::kBatchClasses] = {};
   int threads = 0, smem = 0, grid = 0;
   int tab_off = -1;  // float offset of the shared-memory sponge table, -1 = through L1
   std::vector<int> TJ, IC, stage_floats;
@@ -1236,15 +1237,24 @@ int plan_batch(const lfm_lattice_desc* L, int count, const lfm_batch_tuning& t, 
       j0 = j1;
     }
   }
-  // REAL before COMPLEX, largest first within a level: each free CTA takes
-  // the next item (longest-processing-time order)
+  // By shape class (the REAL classes first), largest first within a class:
+  // each free CTA takes the next item of the class it is on
+  // (longest-processing-time order within the class).
+  std::vector<int> cls(count);
+  for (int l = 0; l < count; ++l) cls[l] = lfm::batch_class_of(L[l].level, L[l].N, plan->TJ[l]);
   std::stable_sort(plan->items.begin(), plan->items.end(),
                    [&](const lfm::BatchItem& a, const lfm::BatchItem& b) {
-                     if (a.level != b.level) return a.level < b.level;
+                     if (cls[a.lattice] != cls[b.lattice]) return cls[a.lattice] < cls[b.lattice];
                      return item_cost(a, L[a.lattice].N) > item_cost(b, L[b.lattice].N);
                    });
   plan->real_items = 0;
-  for (const lfm::BatchItem& it : plan->items) plan->real_items += it.level == LFM_REAL;
+  for (int c = 0; c < lfm::kBatchClasses; ++c) plan->class_off[c] = plan->class_n[c] = 0;
+  for (int k = 0; k < (int)plan->items.size(); ++k) {
+    const lfm::BatchItem& it = plan->items[k];
+    plan->real_items += it.level == LFM_REAL;
+    const int c = cls[it.lattice];
+    if (plan->class_n[c]++ == 0) plan->class_off[c] = k;
+  }
   plan->threads = threads;
   plan->smem = t.stages * max_stage * (int)sizeof(float);
   // The sponge tables (one lattice's at a time) after the largest ring, when
@@ -1277,8 +1287,9 @@ struct lfm_batch {
   int tab_off = -1;
   lfm::BatchLattice* d_lat = nullptr;
   lfm::BatchItem* d_items = nullptr;
-  int* d_counters = nullptr;  // next REAL item, next COMPLEX item, retired CTAs
+  int* d_counters = nullptr;  // next item of each shape class, then retired CTAs
   int nitems = 0, real_items = 0, threads = 0, smem = 0, grid = 0;
+  int class_off[lfm::kBatchClasses] = {}, class_n[lfm::kBatchClasses] = {};
 };
 
 extern "C" {
@@ -1375,6 +1386,10 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
   B->tab_off = plan.tab_off;
   B->nitems = (int)plan.items.size();
   B->real_items = plan.real_items;
+  for (int c = 0; c < lfm::kBatchClasses; ++c) {
+    B->class_off[c] = plan.class_off[c];
+    B->class_n[c] = plan.class_n[c];
+  }
   B->threads = plan.threads;
   B->smem = plan.smem;
   B->grid = plan.grid;
@@ -1386,8 +1401,9 @@ int lfm_batch_create(const lfm_lattice_desc* lattices, int count,
   if (e == cudaSuccess)
     e = cudaMemcpy(B->d_items, plan.items.data(), sizeof(lfm::BatchItem) * plan.items.size(),
                    cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&B->d_counters, 3 * sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(B->d_counters, 0, 3 * sizeof(int));
+  const size_t counters = (lfm::kBatchClasses + 1) * sizeof(int);
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_counters, counters);
+  if (e == cudaSuccess) e = cudaMemset(B->d_counters, 0, counters);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     lfm_batch_destroy(B);
@@ -1408,13 +1424,17 @@ int lfm_batch_step(lfm_batch* batch, int parity, int damp_prev, void* stream) {
   P.items = batch->d_items;
   P.nitems = batch->nitems;
   P.real_items = batch->real_items;
+  for (int c = 0; c < lfm::kBatchClasses; ++c) {
+    P.class_off[c] = batch->class_off[c];
+    P.class_n[c] = batch->class_n[c];
+  }
   P.parity = parity;
   P.damp_prev = damp_prev ? 1 : 0;
   P.stages = batch->stages;
   P.tab_off = batch->tab_off;
   P.status = status;
   P.next_item = batch->d_counters;
-  P.retired = batch->d_counters + 2;
+  P.retired = batch->d_counters + lfm::kBatchClasses;
   cudaError_t e = lfm::launch_batch_step(P, batch->threads, batch->smem, batch->grid,
                                          static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(e, "batch step launch");

@@ -54,6 +54,7 @@ struct TmaParams {
   int pf_mask;                   // index of the mask point field, -1 = lookup table
   int pf_sa;                     // index of S_a colour 0, -1 = none
   int N, TJ, IC, S, JT;
+  int TJL;  // rows of the stage layout: TJ, or a batch lattice's largest tile for a shorter one
   int stage_floats;
   int tab_off;  // float offset of the shared-memory sponge table's tab[0], -1 = read through L1
 };
@@ -502,10 +503,12 @@ __device__ __forceinline__ void color_plane(const TmaParams& P, const float* sme
 // one-row halo copies.  Measured with identical bits: COMPLEX +4 % at 256^3
 // and 512^3, the compensated REAL step +1.5 %; the plain REAL step -0.5 % and
 // the COLOR stencil -3.6 %, so those keep the separate halo copies.
+// The stage layout has room for TJL tile rows (TJL >= TJ: a batch item shorter
+// than its lattice's largest tile leaves the last rows of each field unused).
 template <bool SLAB = true, bool PT = true, bool ONE = false>
 __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uint64_t* bars,
                                             int u, int i0, int i1, int j0) {
-  const int N = P.N, TJ = P.TJ;
+  const int N = P.N, TJ = P.TJ, TJL = P.TJL;
   const int p = i0 - 1 + u;
   const int pw = (SLAB && P.a.slab) ? p : (p % N + N) % N;  // slabs read their ghost planes
   const int s = u % P.S;
@@ -520,7 +523,7 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
   const int64_t plane = (int64_t)pw * N;
   const bool contiguous = ONE && j0 > 0 && j0 + TJ < N;
   for (int f = 0; f < P.ns; ++f) {
-    float* d = st + (size_t)f * (TJ + 2) * N;
+    float* d = st + (size_t)f * (TJL + 2) * N;
     const float* g = P.sf[f];
     if (contiguous) {
       bulk_copy_g2s(d, g + (plane + j0 - 1) * N, row_bytes * (TJ + 2), &bars[s]);
@@ -531,9 +534,9 @@ __device__ __forceinline__ void issue_plane(const TmaParams& P, float* smem, uin
     }
   }
   if (point) {
-    float* base = st + (size_t)P.ns * (TJ + 2) * N;
+    float* base = st + (size_t)P.ns * (TJL + 2) * N;
     for (int g = 0; g < P.np; ++g)
-      bulk_copy_g2s(base + (size_t)g * TJ * N, P.pf[g] + (plane + j0) * N, row_bytes * TJ,
+      bulk_copy_g2s(base + (size_t)g * TJL * N, P.pf[g] + (plane + j0) * N, row_bytes * TJ,
                     &bars[s]);
   }
 }
@@ -768,11 +771,27 @@ struct GeomRTT {
   static constexpr int kStages = 0;    // stage count known at run time only
   static constexpr int TAB = -1;       // the sponge table's place comes with the parameters
   static constexpr int kTabMode = TABM;
-  int N, TJ, S, SF;
+  int N, TJ, S, SF;  // TJ: the stage layout's rows
   __device__ __forceinline__ explicit GeomRTT(const TmaParams& P)
-      : N(P.N), TJ(P.TJ), S(P.S), SF(P.stage_floats) {}
+      : N(P.N), TJ(P.TJL), S(P.S), SF(P.stage_floats) {}
 };
 using GeomRT = GeomRTT<0>;
+
+// A batch lattice shape fixed at compile time: row length N and the layout's
+// TJ rows (the lattice's largest tile; its shorter tiles leave rows unused),
+// so every shared-memory offset of a plane but the stage base is an
+// immediate.  The ring depth stays a run-time value.
+template <int N_, int TJ_, int NS_, int TABM>
+struct GeomBT {
+  static constexpr bool kFixed = false;
+  static constexpr bool kSlab = false;
+  static constexpr int kStages = 0;
+  static constexpr int TAB = -1;
+  static constexpr int kTabMode = TABM;
+  static constexpr int N = N_, TJ = TJ_, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
+  int S;
+  __device__ __forceinline__ explicit GeomBT(const TmaParams& P) : S(P.S) {}
+};
 
 template <int N_, int TJ_, int NS_, int S_ = 3>
 struct GeomCT {
@@ -1254,17 +1273,18 @@ __device__ __forceinline__ void batch_params(TmaParams& P, const BatchLattice& L
   P.pf_sa = -1;
   P.N = L.N;
   P.TJ = rows;
+  P.TJL = L.TJ;  // a shorter tile keeps the lattice's stage layout
   P.IC = L.IC;
   P.S = B.stages;
   P.JT = (L.N + L.TJ - 1) / L.TJ;
-  // a ragged tile's stages are smaller than the lattice's full ones (ns = np)
-  P.stage_floats = rows == L.TJ ? L.stage_floats : L.N * (2 * P.ns * rows + 2 * P.ns);
+  P.stage_floats = L.stage_floats;
   P.tab_off = B.tab_off;  // after the largest ring of the batch, or -1
 }
 
-// The item loop of one level: CTAs take items through that level's counter.
-template <int LEVEL, int V, int TABM>
-__device__ __forceinline__ void batch_level(const BatchParams& B, const BatchItem* items,
+// The item loop of one shape class: CTAs take the class's items through its
+// counter and march each with the class's geometry G.
+template <int LEVEL, int V, class G>
+__device__ __forceinline__ void batch_class(const BatchParams& B, const BatchItem* items,
                                             int nitems, int* next_item, float* smem,
                                             uint64_t* bars, QShared& sh, TmaParams& P,
                                             int& s_item) {
@@ -1280,7 +1300,7 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
       batch_params<LEVEL>(P, L, B, it.j1 - it.j0);
     }
     __syncthreads();  // P is visible to every thread
-    q_march<LEVEL, V, kPlain, true, GeomRTT<TABM>>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
+    q_march<LEVEL, V, kPlain, true, G>(P, smem, bars, sh, it.j0, it.i0, it.i1, P.TJ);
     __syncthreads();  // every wait of the march is over
     if (sh.abort_flag) break;  // same value in every thread
     if (threadIdx.x == 0)
@@ -1288,32 +1308,42 @@ __device__ __forceinline__ void batch_level(const BatchParams& B, const BatchIte
   }
 }
 
-// Every CTA drains the REAL list, then the COMPLEX list: a CTA done with
-// the REAL items starts on the COMPLEX ones at once, so the launch has a
-// single tail (the smallest COMPLEX items).  The two loops run one after the
-// other, so their register demands do not add up.  TABM: the sponge tables in
-// shared memory (1, B.tab_off >= 0) or through L1 (-1).
+template <int C, int TABM>
+__device__ __forceinline__ void batch_run_class(const BatchParams& B, float* smem,
+                                                uint64_t* bars, QShared& sh, TmaParams& P,
+                                                int& s_item) {
+  constexpr BatchShape K = kBatchShapes[C];
+  constexpr int V = K.level == LFM_REAL ? 4 : 2;
+  using G = std::conditional_t<K.N == 0, GeomRTT<TABM>,
+                               GeomBT<(K.N ? K.N : 4), (K.TJ ? K.TJ : 1),
+                                      QFields<K.level>::ns, TABM>>;
+  __syncthreads();
+  if (!sh.abort_flag && B.class_n[C] > 0)
+    batch_class<K.level, V, G>(B, B.items + B.class_off[C], B.class_n[C], B.next_item + C,
+                               smem, bars, sh, P, s_item);
+  if constexpr (C + 1 < kBatchClasses) batch_run_class<C + 1, TABM>(B, smem, bars, sh, P, s_item);
+}
+
+// Every CTA drains the shape classes (kBatchShapes) in order, each through
+// its own loop with its own geometry: a CTA done with one class starts on
+// the next at once, so the launch has a single tail (the smallest COMPLEX
+// items).  The class loops run one after the other, so their register
+// demands do not add up.  TABM: the sponge tables in shared memory
+// (1, B.tab_off >= 0) or through L1 (-1).
 template <int TABM>
-__global__ void __launch_bounds__(512) tma_batch_kernel(const __grid_constant__ BatchParams B) {
+__global__ void __launch_bounds__(512, 1) tma_batch_kernel(const __grid_constant__ BatchParams B) {
   extern __shared__ __align__(128) float smem[];
   __shared__ __align__(8) uint64_t bars[kMaxStages];
   __shared__ QShared sh;
   __shared__ TmaParams P;
   __shared__ int s_item;
   sh.abort_flag = 0;
-  if (B.real_items > 0)
-    batch_level<LFM_REAL, 4, TABM>(B, B.items, B.real_items, B.next_item, smem, bars, sh, P,
-                                   s_item);
-  __syncthreads();
-  if (!sh.abort_flag && B.nitems > B.real_items)
-    batch_level<LFM_COMPLEX, 2, TABM>(B, B.items + B.real_items, B.nitems - B.real_items,
-                                B.next_item + 1, smem, bars, sh, P, s_item);
+  batch_run_class<0, TABM>(B, smem, bars, sh, P, s_item);
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(B.retired, 1) == (int)gridDim.x - 1) {
       // every CTA has taken its last item: rewind for the next launch
-      atomicExch(B.next_item, 0);
-      atomicExch(B.next_item + 1, 0);
+      for (int c = 0; c < kBatchClasses; ++c) atomicExch(B.next_item + c, 0);
       atomicExch(B.retired, 0);
     }
   }
@@ -1599,6 +1629,7 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   }
   if (!ch.TJ) return cudaErrorNotSupported;
   P.TJ = ch.TJ;
+  P.TJL = ch.TJ;
   P.S = ch.S;
   P.IC = ch.IC;
   P.JT = P.N / ch.TJ;

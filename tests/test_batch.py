@@ -52,6 +52,25 @@ def check_coverage(configs, items):
     assert all((a == 1).all() for a in cov.values())
 
 
+# The batch's shape classes (csrc/lfm_batch.h, kBatchShapes): level, N, largest tile.
+SHAPES = [(0, 96, 10), (0, 80, 12), (0, 64, 16), (0, 48, 16), (0, 32, 32), (0, 0, 0),
+          (1, 96, 5), (1, 80, 6), (1, 64, 8), (1, 48, 10), (1, 32, 16), (1, 0, 0)]
+
+
+def shape_class(cfg, threads):
+    """The class a lattice's items run in: its (level, N, largest tile) as the planner cuts
+    it (as few row tiles as the CTA allows, rows as even as possible), else its level's
+    run-time class."""
+    level, N = int(cfg.field_level), cfg.grid_size
+    tpr = N // (4 if level == 0 else 2)
+    tiles = -(-N // (threads // tpr))
+    TJ = -(-N // tiles)
+    for c, (lv, n, tj) in enumerate(SHAPES):
+        if lv == level and (n, tj) == (N, TJ):
+            return c
+    return 5 if level == 0 else 11
+
+
 # ---------------------------------------------------------------- host only
 @pytest.mark.parametrize("tuning", [None, dict(threads=128), dict(stages=5, item_cells=4096),
                                     dict(threads=512, item_cells=1 << 20)])
@@ -65,11 +84,15 @@ def test_plan_covers_every_cell_once(lib, tuning):
     threads, smem, grid = p["launch"]
     assert threads % 32 == 0 and 0 < threads <= (tuning or {}).get("threads", 256)
     assert 0 < smem <= 226 * 1024 and 0 < grid
-    # REAL items first, then COMPLEX; each level runs largest items first
+    # REAL items first, then COMPLEX; grouped by shape class, each class's
+    # largest items first
     it = p["items"]
     assert (np.diff(it[:, 0]) >= 0).all()
-    for lvl in (0, 1):
-        sub = it[it[:, 0] == lvl]
+    threads = (tuning or {}).get("threads", 256)
+    cls = np.array([shape_class(cfgs[l], threads) for l in it[:, 1]])
+    assert (np.diff(cls) >= 0).all()
+    for c in np.unique(cls):
+        sub = it[cls == c]
         N = np.array([cfgs[l].grid_size for l in sub[:, 1]])
         cost = (sub[:, 3] - sub[:, 2]) * N * (sub[:, 5] - sub[:, 4])
         assert (np.diff(cost) <= 0).all()
@@ -86,6 +109,8 @@ def test_plan_of_the_sweep_workload(lib):
     check_coverage(cfgs, p["items"])
     threads, smem, grid = p["launch"]
     assert grid == 296
+    # at 256 threads every lattice of the sweep has a compile-time shape class
+    assert all(shape_class(c, 256) not in (5, 11) for c in cfgs)
 
 
 @pytest.mark.parametrize("bad, code", [(dict(N=10), 3), (dict(level=2), 3), (dict(N=4), 3)])
