@@ -5,9 +5,11 @@ The reference runs a parameter sweep one ``Simulation`` after another
 lattices leave most of a B200 idle that way.  ``BatchedLattices`` holds every
 lattice of a sweep resident in one device arena and advances all of them with
 one persistent kernel launch per step (lfm_batch_step): the CTAs take
-(lattice, row tile, plane chunk) items from a cost-sorted work list, each
-marched exactly like the fused single-lattice kernel, so every lattice's
-result is bit-for-bit the one ``Evolver`` gives for it alone.
+(lattice, row tile, plane chunk) items from a work list grouped by lattice
+shape (the sweep's shapes at 256 threads run with their geometry fixed at
+compile time) and sorted by cost within each group, each marched exactly like
+the fused single-lattice kernel, so every lattice's result is bit-for-bit the
+one ``Evolver`` gives for it alone.
 
 Lattices may differ in N (multiples of 4), level (REAL or COMPLEX), sponge
 and every coupling constant.  ``evolve`` replays a captured CUDA graph of a
