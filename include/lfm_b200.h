@@ -359,7 +359,8 @@ int lfm_batch_destroy(lfm_batch* batch);
 /* The plan lfm_batch_create would make, on the host only (no device needed;
  * 128 registers per thread and `sms` SMs assumed, 148 when sms <= 0).
  * items_out: 6 int32 per item (level, lattice, j0, j1, i0, i1) in the order
- * CTAs take them (REAL first); launch_out: (threads, smem, grid).
+ * CTAs take them (grouped by lattice shape, the REAL shapes first, largest
+ * items first within a shape); launch_out: (threads, smem, grid).
  * Either may be NULL;
  * nitems_out gets the item count. */
 int lfm_batch_plan(const lfm_lattice_desc* lattices, int count, const lfm_batch_tuning* tuning,
