@@ -52,9 +52,22 @@ def check_coverage(configs, items):
     assert all((a == 1).all() for a in cov.values())
 
 
-# The batch's shape classes (csrc/lfm_batch.h, kBatchShapes): level, N, largest tile.
-SHAPES = [(0, 96, 10), (0, 80, 12), (0, 64, 16), (0, 48, 16), (0, 32, 32), (0, 0, 0),
-          (1, 96, 5), (1, 80, 6), (1, 64, 8), (1, 48, 10), (1, 32, 16), (1, 0, 0)]
+def _batch_shapes():
+    """The batch's shape classes (level, N, largest tile), read from kBatchShapes in
+    csrc/lfm_batch.h so the test follows the kernel's table."""
+    import re
+    from pathlib import Path
+
+    src = (Path(__file__).resolve().parents[1] / "lfm-physics_b200" / "csrc" /
+           "lfm_batch.h").read_text()
+    body = src[src.index("kBatchShapes[kBatchClasses] = {"):]
+    body = body[:body.index("};")]
+    lv = {"LFM_REAL": 0, "LFM_COMPLEX": 1}
+    return [(lv[a], int(b), int(c))
+            for a, b, c in re.findall(r"\{(LFM_\w+),\s*(\d+),\s*(\d+)\}", body)]
+
+
+SHAPES = _batch_shapes()
 
 
 def shape_class(cfg, threads):
@@ -68,7 +81,11 @@ def shape_class(cfg, threads):
     for c, (lv, n, tj) in enumerate(SHAPES):
         if lv == level and (n, tj) == (N, TJ):
             return c
-    return 5 if level == 0 else 11
+    return next(c for c, (lv, n, _) in enumerate(SHAPES) if lv == level and n == 0)
+
+
+def test_shape_table_parsed():
+    assert len(SHAPES) == 12 and sum(n == 0 for _, n, _ in SHAPES) == 2
 
 
 # ---------------------------------------------------------------- host only
@@ -110,7 +127,8 @@ def test_plan_of_the_sweep_workload(lib):
     threads, smem, grid = p["launch"]
     assert grid == 296
     # at 256 threads every lattice of the sweep has a compile-time shape class
-    assert all(shape_class(c, 256) not in (5, 11) for c in cfgs)
+    rt = {c for c, (_, n, _) in enumerate(SHAPES) if n == 0}
+    assert all(shape_class(c, 256) not in rt for c in cfgs)
 
 
 @pytest.mark.parametrize("bad, code", [(dict(N=10), 3), (dict(level=2), 3), (dict(N=4), 3)])
