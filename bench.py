@@ -333,7 +333,7 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
                                                      "lfm_b200_bench_tune.json"))
     if args.batch_tuning in ("auto", "default"):
         tuning = "auto" if args.batch_tuning == "auto" else None
-        fixed = dict(threads=256, stages=3, item_cells=65536)
+        fixed = dict(threads=256, stages=5, item_cells=131072)  # the library's default
     else:
         t, s_, c_ = (int(x) for x in args.batch_tuning.split(","))
         tuning = fixed = dict(threads=t, stages=s_, item_cells=c_)
@@ -399,7 +399,7 @@ def run_batched(args, be, dev, rank, barrier, max_over_ranks, peak):
             "autotune": {"best": tune["best"], "ms_per_step": tune["ms_per_step"],
                          "default_ms_per_step": next(
                              (t["ms_per_step"] for t in tune.get("trials", [])
-                              if t["tuning"] == dict(threads=256, stages=3, item_cells=65536)),
+                              if t["tuning"] == dict(threads=256, stages=5, item_cells=131072)),
                              None),
                          "trials": len(tune.get("trials", []))}}
 

@@ -340,8 +340,8 @@ typedef struct lfm_lattice_desc {
 
 typedef struct lfm_batch_tuning {
   int32_t threads;      /* cap on the CTA size (multiple of 32, <= 512); 0 = 256 */
-  int32_t stages;       /* shared-memory stages, 3..6; 0 = 3 */
-  int32_t item_cells;   /* target cells per work item; 0 = 65536 */
+  int32_t stages;       /* shared-memory stages, 3..6; 0 = 5 */
+  int32_t item_cells;   /* target cells per work item; 0 = 131072 */
   int32_t ctas_per_sm;  /* persistent CTAs per SM; 0 = as many as fit */
 } lfm_batch_tuning;
 

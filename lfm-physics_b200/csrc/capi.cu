@@ -1160,8 +1160,10 @@ struct BatchPlan {
 
 constexpr int kBatchSmemLimit = 226 * 1024;
 
+// Defaults: the autotuner's pick on the 256-lattice sweep (256 threads, 5
+// stages, 128 k cells per item: 93.7 GCell/s against 85.5 with 3 stages).
 int validate_batch_tuning(const lfm_batch_tuning* in, lfm_batch_tuning* t) {
-  *t = lfm_batch_tuning{256, 3, 65536, 0};
+  *t = lfm_batch_tuning{256, 5, 131072, 0};
   if (in) {
     if (in->threads) t->threads = in->threads;
     if (in->stages) t->stages = in->stages;

@@ -793,11 +793,13 @@ struct GeomBT {
   __device__ __forceinline__ explicit GeomBT(const TmaParams& P) : S(P.S) {}
 };
 
-template <int N_, int TJ_, int NS_, int S_ = 3>
+// SLAB_: the tile may step a slab of planes (one rank's part of a lattice
+// split along i, with its ghost planes); otherwise whole lattices only.
+template <int N_, int TJ_, int NS_, int S_ = 3, bool SLAB_ = false>
 struct GeomCT {
   static_assert(N_ % 2 == 0, "the sponge keys of the compile-time tiles assume even N");
   static constexpr bool kFixed = true;
-  static constexpr bool kSlab = false;  // whole lattices only
+  static constexpr bool kSlab = SLAB_;
   static constexpr int kStages = S_;
   static constexpr int N = N_, TJ = TJ_, S = S_, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
   static constexpr int TAB = S * SF + 3;  // float offset of the sponge table's tab[0]
@@ -862,7 +864,7 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   float mask[V], absorb[V];
   if constexpr (G::kFixed) {
     // the compile-time tiles never stream the mask; their table sits at TAB
-    tab_mask<V>(smem + G::TAB, qterm(i, N), N, K, mask);
+    tab_mask<V>(smem + G::TAB, qterm(i + (G::kSlab ? a.i_off : 0), N), N, K, mask);
   } else if (P.pf_mask >= 0) {  // the streamed mask, from the centre plane's stage
     const Vec<V> m = lds<V>(smem, bc + L.o_pt + P.pf_mask * PTS);
 #pragma unroll
@@ -1506,18 +1508,18 @@ int KernelSlot<LEVEL, V, QUEUE, MODE>::granted = 0;
 
 // Compile-time tiles for the headline sizes (resident layout); MODE kComp:
 // the compensated (Delta-form) step on the same tile.
-template <int LEVEL, int V, int N, int TJ, int S, int MODE = kPlain>
+template <int LEVEL, int V, int N, int TJ, int S, int MODE = kPlain, bool SLAB = false>
 struct FixedSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
-    return tma_queue_kernel<LEVEL, V, MODE, GeomCT<N, TJ, QFields<LEVEL, MODE>::ns, S>>;
+    return tma_queue_kernel<LEVEL, V, MODE, GeomCT<N, TJ, QFields<LEVEL, MODE>::ns, S, SLAB>>;
   }
 };
-template <int LEVEL, int V, int N, int TJ, int S, int MODE>
-std::mutex FixedSlot<LEVEL, V, N, TJ, S, MODE>::mu;
-template <int LEVEL, int V, int N, int TJ, int S, int MODE>
-int FixedSlot<LEVEL, V, N, TJ, S, MODE>::granted = 0;
+template <int LEVEL, int V, int N, int TJ, int S, int MODE, bool SLAB>
+std::mutex FixedSlot<LEVEL, V, N, TJ, S, MODE, SLAB>::mu;
+template <int LEVEL, int V, int N, int TJ, int S, int MODE, bool SLAB>
+int FixedSlot<LEVEL, V, N, TJ, S, MODE, SLAB>::granted = 0;
 
 // The compile-time tiles: step form, level, cells per lane, N, rows, stages.
 // The compensated step has one at the throughput size; split chi at REAL 256^3
@@ -1546,9 +1548,9 @@ const FixedTile* fixed_tile(int mode, int level, int V, int N) {
   return nullptr;
 }
 
-template <int LEVEL, int V, int N, int TJ, int MODE = kPlain>
+template <int LEVEL, int V, int N, int TJ, int MODE = kPlain, bool SLAB = false>
 cudaError_t launch_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream) {
-  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(MODE, LEVEL, V, N, TJ), MODE>;
+  using Slot = FixedSlot<LEVEL, V, N, TJ, fixed_stages(MODE, LEVEL, V, N, TJ), MODE, SLAB>;
   return launch_kernel(Slot::fn(), &Slot::granted, &Slot::mu, P, ch, stream);
 }
 
@@ -1562,11 +1564,20 @@ int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
 // in shared memory (ch.smem includes the table then); false if not.
 template <int LEVEL, int V, int MODE = kPlain>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
-  if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0 || P.a.slab) return false;
+  if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0) return false;
   const FixedTile* t = fixed_tile(MODE, LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
   if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
     return false;
+  if (P.a.slab) {
+    // a rank's slab of a lattice split along i: the plain 512^3 tiles
+    if constexpr (MODE == kPlain && LEVEL == LFM_REAL && V == 4) {
+      if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 4, kPlain, true>(P, ch, stream); return true; }
+    } else if constexpr (MODE == kPlain && LEVEL == LFM_COMPLEX && V == 2) {
+      if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 2, kPlain, true>(P, ch, stream); return true; }
+    }
+    return false;
+  }
   if constexpr (MODE == kSplit) {
     if constexpr (LEVEL == LFM_REAL && V == 2) {
       if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 2, kSplit>(P, ch, stream); return true; }
@@ -1610,7 +1621,8 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // tile (TJ rows, S stages) when its ring and the sponge table fit in shared
   // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
-  const FixedTile* ft = (QUEUE && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns && !P.a.slab)
+  const bool slab_tile = !P.a.slab || (MODE == kPlain && P.N == 512);  // slab variants: 512^3
+  const FixedTile* ft = (QUEUE && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns && slab_tile)
                             ? fixed_tile(MODE, LEVEL, V, P.N) : nullptr;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {

@@ -246,6 +246,36 @@ def test_slabs_match_the_whole_lattice(be, N, world, overlap, level):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("level, overlap", [("real", False), ("real", True), ("complex", False)])
+def test_slabs_of_a_512_lattice_on_the_compile_time_tiles(be, level, overlap):
+    """Two slabs of a 512^3 lattice run on the compile-time 512^3 tiles (their slab
+    variant: ghost planes, the sponge key of the global plane) and agree bit for bit
+    with the whole lattice after 3 steps."""
+    from lfm_b200 import Evolver, _lib
+    from lfm_b200.slab import SlabEvolver, evolve_local, gather_local
+
+    N, world, steps = 512, 2, 3
+    cx = level == "complex"
+    cfg = _cfg(N, cx)
+    E, pi, chi = _state(N, cx, 77)
+    ev = Evolver(cfg, backend=be)
+    _load(ev, E, pi, chi)
+    ev.evolve(steps)
+    want = [ev.get_psi_real(), ev.get_chi()] + ([ev.get_psi_imag()] if cx else [])
+    del ev
+    slabs = [SlabEvolver(cfg, backend=be, rank=r, world=world) for r in range(world)]
+    for sl in slabs:
+        _load(sl, E, pi, chi)
+    evolve_local(slabs, steps, overlap=overlap)
+    got = [gather_local(slabs, "psi_r"), gather_local(slabs, "chi")]
+    if cx:
+        got.append(gather_local(slabs, "psi_i"))
+    for g, w in zip(got, want):
+        assert bits_equal(g, w)
+    assert _lib.device_status() == 0
+
+
+@pytest.mark.gpu
 def test_single_slab_is_the_whole_lattice(be):
     from lfm_b200 import Evolver
     from lfm_b200.slab import SlabEvolver
