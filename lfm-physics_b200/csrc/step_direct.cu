@@ -50,10 +50,10 @@ __global__ void __launch_bounds__(256) direct_step_kernel(const StepArgs a) {
     const S19 X = gather(a.chi, ix);
     const float chi_prev = a.chi_prev[x];
     if (LEVEL != LFM_COLOR && a.split) {
-      // split chi: chi = chi0 + hi + lo (resident slots, previous Psi damped on read)
-      const S19 L = gather(a.chi_lo, ix);
-      const float lapD = lap_split(X, L);
-      const double d = split_value(X.c, L.c);
+      // split chi: chi = chi0 + hi + lo (resident slots, previous Psi damped on read);
+      // the offset's Laplacian is that of hi (lfm_cells.cuh, split chi)
+      const float lapD = lap19_diff(X);
+      const double d = split_value(X.c, a.chi_lo[x]);
       const double d_prev = split_value(chi_prev, a.chi_lo_prev[x]);
       SplitChi c;
       if (LEVEL == LFM_REAL) {

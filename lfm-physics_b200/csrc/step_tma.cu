@@ -752,10 +752,13 @@ __device__ __forceinline__ Faces faces_of(const S19& s) {
   return f;
 }
 
-// Stencil fields of the march: Psi components and chi (split chi: hi, lo).
+// Stencil and point fields of the march: Psi components and chi (split chi:
+// its hi part) in the stencil, their previous values (and split chi's lo and
+// lo_prev) as point fields.
 template <int LEVEL, int MODE = kPlain>
 struct QFields {
-  static constexpr int ns = ((LEVEL == LFM_REAL) ? 2 : 3) + (MODE == kSplit ? 1 : 0);
+  static constexpr int ns = (LEVEL == LFM_REAL) ? 2 : 3;     // Psi components, chi (hi)
+  static constexpr int np = ns + (MODE == kSplit ? 2 : 0);  // their previous; split: lo, lo_prev
 };
 
 // Tile geometry of a march.  GeomRT reads it from the parameters (any
@@ -795,13 +798,13 @@ struct GeomBT {
 
 // SLAB_: the tile may step a slab of planes (one rank's part of a lattice
 // split along i, with its ghost planes); otherwise whole lattices only.
-template <int N_, int TJ_, int NS_, int S_ = 3, bool SLAB_ = false>
+template <int N_, int TJ_, int NS_, int S_ = 3, bool SLAB_ = false, int NP_ = NS_>
 struct GeomCT {
   static_assert(N_ % 2 == 0, "the sponge keys of the compile-time tiles assume even N");
   static constexpr bool kFixed = true;
   static constexpr bool kSlab = SLAB_;
   static constexpr int kStages = S_;
-  static constexpr int N = N_, TJ = TJ_, S = S_, SF = N_ * (NS_ * (TJ_ + 2) + NS_ * TJ_);
+  static constexpr int N = N_, TJ = TJ_, S = S_, SF = N_ * (NS_ * (TJ_ + 2) + NP_ * TJ_);
   static constexpr int TAB = S * SF + 3;  // float offset of the sponge table's tab[0]
   static constexpr int kTabMode = 1;
   __device__ __forceinline__ explicit GeomCT(const TmaParams&) {}
@@ -880,21 +883,22 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
   for (int e = 0; e < V; ++e) absorb[e] = fsub(1.0f, mask[e]);
   const int64_t gofs = ((int64_t)i * N + j) * N + k0;
   if constexpr (MODE == kSplit) {
-    // Split chi: stencil fields Psi (Psi_r, Psi_i), hi, lo; point fields their
-    // previous slots in the same order.  New values go over the previous slots.
+    // Split chi: stencil fields Psi (Psi_r, Psi_i), hi; point fields their
+    // previous slots in the same order, then lo and lo_prev.  New values go
+    // over the previous slots.
     if constexpr (LEVEL == LFM_REAL) {
       const Vec<V> ep = lds<V>(smem, bc + L.o_pt);
       const Vec<V> hp = lds<V>(smem, bc + L.o_pt + PTS);
-      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+      const Vec<V> lc = lds<V>(smem, bc + L.o_pt + 2 * PTS);
+      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 3 * PTS);
       float o_e[V], o_h[V], o_l[V];
 #pragma unroll
       for (int e = 0; e < V; ++e) {
         const S19 E = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
         const S19 H = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
-        const S19 Lo = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
         const float epv = a.damp_prev ? fmul(ep.v[e], absorb[e]) : ep.v[e];
         const RealSplit o =
-            real_cell_split(lap19_fma(E), E.c, epv, lap_split(H, Lo), split_value(H.c, Lo.c),
+            real_cell_split(lap19_fma(E), E.c, epv, lap19_diff(H), split_value(H.c, lc.v[e]),
                             split_value(hp.v[e], lp.v[e]), mask[e], absorb[e], a.c);
         o_e[e] = o.psi; o_h[e] = o.chi.hi; o_l[e] = o.chi.lo;
       }
@@ -905,19 +909,19 @@ __device__ __forceinline__ bool q_plane(const TmaParams& P, float* smem, uint64_
       const Vec<V> rp = lds<V>(smem, bc + L.o_pt);
       const Vec<V> ip = lds<V>(smem, bc + L.o_pt + PTS);
       const Vec<V> hp = lds<V>(smem, bc + L.o_pt + 2 * PTS);
-      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 3 * PTS);
+      const Vec<V> lc = lds<V>(smem, bc + L.o_pt + 3 * PTS);
+      const Vec<V> lp = lds<V>(smem, bc + L.o_pt + 4 * PTS);
       float o_r[V], o_i[V], o_h[V], o_l[V];
 #pragma unroll
       for (int e = 0; e < V; ++e) {
         const S19 R = q_s19<V>(Q[0][PA], Q[0][PB], Q[0][PC], e);
         const S19 I = q_s19<V>(Q[1][PA], Q[1][PB], Q[1][PC], e);
         const S19 H = q_s19<V>(Q[2][PA], Q[2][PB], Q[2][PC], e);
-        const S19 Lo = q_s19<V>(Q[3][PA], Q[3][PB], Q[3][PC], e);
         const float rpv = a.damp_prev ? fmul(rp.v[e], absorb[e]) : rp.v[e];
         const float ipv = a.damp_prev ? fmul(ip.v[e], absorb[e]) : ip.v[e];
         const ComplexSplit o = complex_cell_split(
             lap19_fma(R), R.c, rpv, faces_of(R), lap19_fma(I), I.c, ipv, faces_of(I),
-            lap_split(H, Lo), split_value(H.c, Lo.c), split_value(hp.v[e], lp.v[e]), mask[e],
+            lap19_diff(H), split_value(H.c, lc.v[e]), split_value(hp.v[e], lp.v[e]), mask[e],
             absorb[e], a.c);
         o_r[e] = o.pr; o_i[e] = o.pi; o_h[e] = o.chi.hi; o_l[e] = o.chi.lo;
       }
@@ -1513,7 +1517,8 @@ struct FixedSlot {
   static std::mutex mu;
   static int granted;
   static auto fn() {
-    return tma_queue_kernel<LEVEL, V, MODE, GeomCT<N, TJ, QFields<LEVEL, MODE>::ns, S, SLAB>>;
+    using F = QFields<LEVEL, MODE>;
+    return tma_queue_kernel<LEVEL, V, MODE, GeomCT<N, TJ, F::ns, S, SLAB, F::np>>;
   }
 };
 template <int LEVEL, int V, int N, int TJ, int S, int MODE, bool SLAB>
@@ -1564,7 +1569,9 @@ int sponge_table_bytes(int count) { return (4 * (count + 5) + 15) / 16 * 16; }
 // in shared memory (ch.smem includes the table then); false if not.
 template <int LEVEL, int V, int MODE = kPlain>
 bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t* err) {
-  if (P.np != P.ns || P.pf_mask >= 0 || P.pf_sa >= 0) return false;
+  if (P.np != QFields<LEVEL, MODE>::np || P.ns != QFields<LEVEL, MODE>::ns || P.pf_mask >= 0 ||
+      P.pf_sa >= 0)
+    return false;
   const FixedTile* t = fixed_tile(MODE, LEVEL, V, P.N);
   if (!t || t->TJ != ch.TJ || t->S != ch.S) return false;
   if (ch.smem != t->S * stage_bytes(P.N, ch.TJ, P.ns, P.np) + sponge_table_bytes(P.a.lut.count))
@@ -1622,7 +1629,8 @@ cudaError_t plan_and_launch(TmaParams& P, const TileConfig* forced, cudaStream_t
   // memory; the planner still picks the plane chunk.
   TileConfig fixed_cfg;
   const bool slab_tile = !P.a.slab || (MODE == kPlain && P.N == 512);  // slab variants: 512^3
-  const FixedTile* ft = (QUEUE && P.pf_mask < 0 && P.pf_sa < 0 && P.np == P.ns && slab_tile)
+  const bool resident = P.ns == QFields<LEVEL, MODE>::ns && P.np == QFields<LEVEL, MODE>::np;
+  const FixedTile* ft = (QUEUE && P.pf_mask < 0 && P.pf_sa < 0 && resident && slab_tile)
                             ? fixed_tile(MODE, LEVEL, V, P.N) : nullptr;
   if (ft && ft->S * stage_bytes(P.N, ft->TJ, P.ns, P.np) + tab_smem > kSmemLimit) ft = nullptr;
   if (!forced && ft) {
@@ -1694,7 +1702,8 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
   P.pf_sa = -1;
   const int64_t n3 = (int64_t)N * N * N;
   if (a.split) {
-    // split chi: stencil fields Psi..., hi, lo; point fields their previous slots
+    // split chi: stencil fields Psi..., hi; point fields their previous slots,
+    // then lo and lo_prev
     if (a.level == LFM_COLOR || a.comp || a.mask || !a.chi_lo || !a.chi_lo_prev ||
         !a.chi_lo_out)
       return cudaErrorNotSupported;
@@ -1702,8 +1711,10 @@ cudaError_t launch_tma_step(const StepArgs& a, cudaStream_t stream) {
     P.sf[f] = a.pr; P.pf[f++] = a.pr_prev;
     if (a.level == LFM_COMPLEX) { P.sf[f] = a.pi; P.pf[f++] = a.pi_prev; }
     P.sf[f] = a.chi; P.pf[f++] = a.chi_prev;
-    P.sf[f] = a.chi_lo; P.pf[f++] = a.chi_lo_prev;
-    P.ns = P.np = f;
+    P.ns = f;
+    P.pf[f++] = a.chi_lo;
+    P.pf[f++] = a.chi_lo_prev;
+    P.np = f;
   } else if (a.level == LFM_REAL) {
     P.ns = 2;
     P.sf[0] = a.pr; P.sf[1] = a.chi;
