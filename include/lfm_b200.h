@@ -211,7 +211,8 @@ int lfm_leapfrog_complex_comp_f32(const float* psi_r, float* psi_r_next, float* 
  * chi is held as chi0 + hi + lo, two float32 slots per time level (hi, and lo
  * the part below one ulp of hi); Psi as in the plain resident step.  The chi
  * update and every acceleration term involving chi run in float64, the
- * Laplacians in float32 (hi's from neighbour differences).  The slots rotate
+ * Laplacians in float32 (chi's is hi's, from neighbour differences; lo enters
+ * the step at the cell only).  The slots rotate
  * as in lfm_leapfrog_real_f32: each call reads (cur, prev) of every field and
  * writes the new values over prev; damp_prev as there (Psi's previous slot is
  * multiplied by (1 - mask) on read).  chi's previous slots are undamped.
