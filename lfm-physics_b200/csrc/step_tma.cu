@@ -1527,8 +1527,8 @@ template <int LEVEL, int V, int N, int TJ, int S, int MODE, bool SLAB>
 int FixedSlot<LEVEL, V, N, TJ, S, MODE, SLAB>::granted = 0;
 
 // The compile-time tiles: step form, level, cells per lane, N, rows, stages.
-// The compensated step has one at the throughput size; split chi at REAL 256^3
-// and 512^3 (its ring is COMPLEX-shaped: three stencil and three point fields).
+// The compensated step has one at the throughput size; split chi at 256^3 and
+// 512^3, two cells per lane (its ring adds chi's lo and lo_prev as point fields).
 struct FixedTile {
   int mode, level, V, N, TJ, S;
 };
@@ -1537,7 +1537,8 @@ constexpr FixedTile kFixedTiles[] = {
     {kPlain, LFM_COMPLEX, 2, 512, 2, 3}, {kPlain, LFM_COMPLEX, 2, 256, 4, 3},
     {kPlain, LFM_REAL, 4, 128, 8, 3},    {kPlain, LFM_COMPLEX, 2, 128, 4, 3},
     {kComp, LFM_REAL, 4, 512, 4, 3},     {kSplit, LFM_REAL, 2, 512, 2, 3},
-    {kSplit, LFM_REAL, 2, 256, 4, 3}};
+    {kSplit, LFM_REAL, 2, 256, 4, 3},    {kSplit, LFM_COMPLEX, 2, 512, 2, 3},
+    {kSplit, LFM_COMPLEX, 2, 256, 4, 3}};
 
 // The stage count of the compile-time tile (mode, level, V, N, TJ); 0 if none.
 constexpr int fixed_stages(int mode, int level, int V, int N, int TJ) {
@@ -1586,7 +1587,7 @@ bool try_fixed(TmaParams& P, const Choice& ch, cudaStream_t stream, cudaError_t*
     return false;
   }
   if constexpr (MODE == kSplit) {
-    if constexpr (LEVEL == LFM_REAL && V == 2) {
+    if constexpr (V == 2) {
       if (P.N == 512) { *err = launch_fixed<LEVEL, V, 512, 2, kSplit>(P, ch, stream); return true; }
       if (P.N == 256) { *err = launch_fixed<LEVEL, V, 256, 4, kSplit>(P, ch, stream); return true; }
     }

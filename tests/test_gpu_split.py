@@ -65,9 +65,9 @@ def _run(be, cfg, E, pi, chi, steps, graphs=True):
 
 
 @pytest.mark.parametrize("level, N", [("real", 32), ("real", 48), ("complex", 32),
-                                      ("complex", 48), ("real", 256)])
+                                      ("complex", 48), ("real", 256), ("complex", 256)])
 def test_fused_and_direct_kernels_agree(be, level, N):
-    """Run-time tiles (32, 48) and the compile-time REAL tile (256) against the direct kernel."""
+    """Run-time tiles (32, 48) and the compile-time tiles (256) against the direct kernel."""
     from lfm_b200 import _lib
     from lfm_b200.config import gravity_em, gravity_only
 
