@@ -488,19 +488,24 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
         st = soliton_state(N, *[t.to(dev).float() for t in pert], sigma, cfg.chi0, None, True,
                            omega_dt=od)
         target = leapfrog(cfg, st, steps, backend=be)[4].clone()
+        st[4] = st[5] = torch.full((N, N, N), cfg.chi0, device=dev, dtype=torch.float64)
+        target_split = leapfrog(cfg, st, steps, backend=be, split_chi=True)[4].clone()
     stream = torch.cuda.current_stream(dev)
 
-    def one(timed: bool):
+    def one(timed: bool, split: bool = False):
         p = [t.clone().requires_grad_(True) for t in params]
-        dchi = torch.zeros((N, N, N), device=dev, requires_grad=True)
-        st = soliton_state(N, *p, sigma, cfg.chi0, dchi, True, omega_dt=od)
+        dchi = torch.zeros((N, N, N), device=dev, requires_grad=True,
+                           dtype=torch.float64 if split else torch.float32)
+        st = soliton_state(N, *p, sigma, cfg.chi0, None if split else dchi, True, omega_dt=od)
+        if split:  # chi in float64: chi0 + hi + lo in the split-chi steps
+            st[4] = st[5] = cfg.chi0 + dchi
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
         torch.cuda.synchronize(dev)
         barrier()
         ev[0].record(stream)
-        out = leapfrog(cfg, st, steps, backend=be)
+        out = leapfrog(cfg, st, steps, backend=be, split_chi=split)
         ev[1].record(stream)
-        loss = ((out[4] - target) ** 2).sum()
+        loss = ((out[4] - (target_split if split else target)) ** 2).sum()
         loss.backward()
         ev[2].record(stream)
         torch.cuda.synchronize(dev)
@@ -530,6 +535,8 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
     torch.cuda.synchronize(dev)
     plain = max_over_ranks(a.elapsed_time(b))
     mem = memory_bytes(cfg, steps)
+    one(False, split=True)
+    sfwd, sbwd, sloss, _ = one(True, split=True)
     return {"workload": f"COMPLEX {N}^3 gravity_em, {steps} steps, two packets + per-cell "
                         "chi offset, loss |chi - chi_target|^2",
             "forward_ms": fwd, "backward_ms": bwd, "backward_over_forward": bwd / fwd,
@@ -537,7 +544,13 @@ def run_adjoint(args, be, dev, barrier, max_over_ranks):
             "loss": loss, "grad_max": dict(zip(("amplitude", "centre", "phase", "dchi"), gmax)),
             "checkpoints": mem["checkpoints"], "checkpoint_bytes": mem["checkpoint_bytes"],
             "segment_bytes": mem["segment_bytes"], "all_states_bytes": mem["all_states_bytes"],
-            "peak_extra_bytes": peak}
+            "peak_extra_bytes": peak,
+            "split_chi": {"how": "leapfrog(split_chi=True): chi as chi0 + hi + lo in the forward "
+                                 "and the recomputed segments, chi and the loss in float64",
+                          "forward_ms": sfwd, "backward_ms": sbwd,
+                          "backward_over_forward": sbwd / sfwd, "loss": sloss,
+                          "checkpoint_bytes": memory_bytes(cfg, steps,
+                                                           split_chi=True)["checkpoint_bytes"]}}
 
 
 def run_b200(args):

@@ -233,6 +233,17 @@ int lfm_leapfrog_complex_split_f32(const float* psi_r, float* psi_r_prev_io, con
                                    double kappa, double lambda_self, double chi0, double e0_sq,
                                    double epsilon_w, void* stream);
 
+/* One split-chi step out of place, as lfm_advance_f32 for the plain step: reads
+ * (cur, prev) of every field, writes the new state to the *_out buffers (the
+ * adjoint's recomputed segments).  damp_prev as in the resident call. */
+int lfm_advance_split_f32(int level, const float* psi_r, const float* psi_r_prev,
+                          float* psi_r_out, const float* psi_i, const float* psi_i_prev,
+                          float* psi_i_out, const float* chi_hi, const float* chi_hi_prev,
+                          float* chi_hi_out, const float* chi_lo, const float* chi_lo_prev,
+                          float* chi_lo_out, const float* mask_table, const lfm_mask_lut* lut,
+                          int damp_prev, int N, double dt2, double kappa, double lambda_self,
+                          double chi0, double e0_sq, double epsilon_w, void* stream);
+
 /* ------------------------------------------------------------------------
  * Poisson equilibration of chi (lfm/fields/equilibrium.py:26-121, as
  * Simulation.equilibrate calls it, lfm/simulation.py:877-963):

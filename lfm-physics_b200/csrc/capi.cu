@@ -981,6 +981,51 @@ int lfm_leapfrog_complex_split_f32(const float* psi_r, float* psi_r_prev_io, con
   return run_step(a, static_cast<cudaStream_t>(stream));
 }
 
+int lfm_advance_split_f32(int level, const float* psi_r, const float* psi_r_prev,
+                          float* psi_r_out, const float* psi_i, const float* psi_i_prev,
+                          float* psi_i_out, const float* chi_hi, const float* chi_hi_prev,
+                          float* chi_hi_out, const float* chi_lo, const float* chi_lo_prev,
+                          float* chi_lo_out, const float* mask_table, const lfm_mask_lut* lut,
+                          int damp_prev, int N, double dt2, double kappa, double lambda_self,
+                          double chi0, double e0_sq, double epsilon_w, void* stream) {
+  if (level != LFM_REAL && level != LFM_COMPLEX)
+    return fail(LFM_ERR_UNSUPPORTED, "advance: level %d (REAL and COMPLEX only)", level);
+  int rc = check_n(N);
+  if (rc) return rc;
+  const bool cx = level == LFM_COMPLEX;
+  if (!psi_r || !psi_r_prev || !psi_r_out || !chi_hi || !chi_hi_prev || !chi_hi_out ||
+      !chi_lo || !chi_lo_prev || !chi_lo_out || (cx && (!psi_i || !psi_i_prev || !psi_i_out)))
+    return fail(LFM_ERR_INVALID_ARG, "null buffer");
+  rc = check_lut(mask_table, lut, N);
+  if (rc) return rc;
+  const size_t b = sizeof(float) * (size_t)N * N * N;
+  std::vector<Span> ins = {{psi_r, b}, {psi_r_prev, b}, {chi_hi, b},
+                           {chi_hi_prev, b}, {chi_lo, b}, {chi_lo_prev, b}};
+  std::vector<Span> outs = {{psi_r_out, b}, {chi_hi_out, b}, {chi_lo_out, b}};
+  if (cx) {
+    ins.push_back({psi_i, b});
+    ins.push_back({psi_i_prev, b});
+    outs.push_back({psi_i_out, b});
+  }
+  rc = check_disjoint(ins, outs);
+  if (rc) return rc;
+  lfm::StepArgs a{};
+  a.level = level;
+  a.N = N;
+  a.split = 1;
+  a.c = lfm::make_step_consts(dt2, kappa, lambda_self, chi0, e0_sq, cx ? epsilon_w : 0.0, 0, 0,
+                              0, 0);
+  a.pr = psi_r; a.pr_prev = psi_r_prev; a.pr_out = psi_r_out;
+  if (cx) {
+    a.pi = psi_i; a.pi_prev = psi_i_prev; a.pi_out = psi_i_out;
+  }
+  a.chi = chi_hi; a.chi_prev = chi_hi_prev; a.chi_out = chi_hi_out;
+  a.chi_lo = chi_lo; a.chi_lo_prev = chi_lo_prev; a.chi_lo_out = chi_lo_out;
+  a.lut = device_lut(mask_table, lut);
+  a.damp_prev = damp_prev ? 1 : 0;
+  return run_step(a, static_cast<cudaStream_t>(stream));
+}
+
 int lfm_helmholtz_sa_f32(lfm_context* ctx, const float* psi_r, const float* psi_i,
                          float* sa_raw, int N, double sa_gamma, double sa_d, void* stream) {
   int rc = check_n(N);

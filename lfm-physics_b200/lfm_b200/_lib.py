@@ -82,6 +82,8 @@ _SIGNATURES = {
     + [_P],
     "lfm_leapfrog_complex_split_f32": [_P] * 9 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6
     + [_P],
+    "lfm_advance_split_f32": [c_int] + [_P] * 13 + [POINTER(MaskLut), c_int, c_int] + [_D] * 6
+    + [_P],
     "lfm_helmholtz_sa_f32": [_P] * 4 + [c_int, _D, _D, _P],
     "lfm_sa_clip_f32": [_P, _P, c_int64, _P],
     "lfm_device_status": [POINTER(c_int), c_int],

@@ -58,6 +58,19 @@ class _Lattice:
         self.common = (float(c.dt) ** 2, float(c.kappa), float(c.lambda_self), float(c.chi0),
                        float(c.e0_sq))
 
+    # the slot tensors of time level i, in the order of a state buffer
+    def slots(self, i: int) -> list:
+        return [self.pr[i], self.pi[i] if self.cx else None, self.chi[i]]
+
+    def new_state_buffers(self) -> list:
+        f32 = dict(dtype=torch.float32, device=self.device)
+        return [torch.empty(self.n, **f32), torch.empty(self.n, **f32) if self.cx else None,
+                torch.empty(self.n, **f32)]
+
+    def chi32(self, st, k: int):
+        """chi of a state buffer as the float32 array the adjoint step linearises at."""
+        return st[2]
+
     # state in the reference representation <-> resident slots
     def load(self, state) -> None:
         self.cur, self.damp = 0, False  # prev slots hold the reference prev (already damped)
@@ -104,13 +117,99 @@ class _Lattice:
                   ctypes.byref(self.desc), int(damp), self.N, *self.common,
                   float(self.config.epsilon_w), _stream_handle(self.device))
 
-    def adjoint_step(self, pr, pi, chi, chi_next, g_out, g_in) -> None:
+    def adjoint_step(self, st, nx, g_out, g_in) -> None:
+        """The gradient back through the step from state buffer st to nx."""
         ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
         go = (ctypes.c_void_p * 6)(*[ptr(t) for t in g_out])
         gi = (ctypes.c_void_p * 6)(*[ptr(t) for t in g_in])
-        _lib.call("lfm_adjoint_step_f32", int(self.level), pr.data_ptr(), ptr(pi),
-                  chi.data_ptr(), chi_next.data_ptr(), self.table.data_ptr(),
+        _lib.call("lfm_adjoint_step_f32", int(self.level), st[0].data_ptr(), ptr(st[1]),
+                  self.chi32(st, 0).data_ptr(), self.chi32(nx, 1).data_ptr(),
+                  self.table.data_ptr(),
                   ctypes.byref(self.desc), go, gi, self.N, *self.common,
+                  float(self.config.epsilon_w), _stream_handle(self.device))
+
+
+class _SplitLattice(_Lattice):
+    """The same lattice with chi held as chi0 + hi + lo (the split-chi step,
+    lfm_leapfrog_*_split_f32): the forward and the recomputed segments carry
+    chi to about 48 bits, and chi comes out in float64.  A state buffer is
+    (psi_r, psi_i, hi, lo); the adjoint step linearises at chi0 + hi rounded to
+    float32 (within one ulp of chi), the same float32 arithmetic as for the
+    plain step.  It finds cells held by the
+    clamp chi >= -chi0 from that float32 chi, so a clamped cell may be missed
+    (the packets of the adjoint workload stay far from the clamp)."""
+
+    def __init__(self, config, backend: B200Backend) -> None:
+        super().__init__(config, backend)
+        f32 = dict(dtype=torch.float32, device=self.device)
+        self.lo = [torch.empty(self.n, **f32) for _ in range(2)]
+        self.chi_f32 = [torch.empty(self.n, **f32) for _ in range(2)]
+        self.chi0 = float(config.chi0)
+
+    def slots(self, i: int) -> list:
+        return [self.pr[i], self.pi[i] if self.cx else None, self.chi[i], self.lo[i]]
+
+    def new_state_buffers(self) -> list:
+        return super().new_state_buffers() + [
+            torch.empty(self.n, dtype=torch.float32, device=self.device)]
+
+    def chi32(self, st, k: int):
+        # chi0 + hi in float32: within one ulp of float32(chi0 + hi + lo), one launch
+        return torch.add(st[2], self.chi0, out=self.chi_f32[k])
+
+    def _split(self, chi, hi, lo) -> None:
+        d = chi.reshape(-1).to(torch.float64) - self.chi0
+        h = d.to(torch.float32)
+        hi.copy_(h)
+        lo.copy_(d - h.double())
+
+    def _chi64(self, hi, lo):
+        return self.chi0 + hi.double() + lo.double()
+
+    def load(self, state) -> None:
+        super().load([state[0], state[1], state[2], state[3], state[4].float(),
+                      state[5].float()])
+        self._split(state[4], self.chi[0], self.lo[0])
+        self._split(state[5], self.chi[1], self.lo[1])
+
+    def state(self) -> list:
+        out = super().state()
+        c, p = self.cur, 1 - self.cur
+        out[4] = self._chi64(self.chi[c], self.lo[c])
+        out[5] = self._chi64(self.chi[p], self.lo[p])
+        return out
+
+    def _split_step(self, cur, prev_io, damp: bool) -> None:
+        """One split step: reads cur and prev_io (slot lists), writes the new state over
+        prev_io."""
+        stream = _stream_handle(self.device)
+        tab, desc = self.table.data_ptr(), ctypes.byref(self.desc)
+        if self.cx:
+            _lib.call("lfm_leapfrog_complex_split_f32", cur[0].data_ptr(),
+                      prev_io[0].data_ptr(), cur[1].data_ptr(), prev_io[1].data_ptr(),
+                      cur[2].data_ptr(), prev_io[2].data_ptr(), cur[3].data_ptr(),
+                      prev_io[3].data_ptr(), tab, desc, int(damp), self.N, *self.common,
+                      float(self.config.epsilon_w), stream)
+        else:
+            _lib.call("lfm_leapfrog_real_split_f32", cur[0].data_ptr(), prev_io[0].data_ptr(),
+                      cur[2].data_ptr(), prev_io[2].data_ptr(), cur[3].data_ptr(),
+                      prev_io[3].data_ptr(), tab, desc, int(damp), self.N, *self.common,
+                      stream)
+
+    def step(self) -> None:
+        c, p = self.cur, 1 - self.cur
+        self._split_step(self.slots(c), self.slots(p), self.damp)
+        self.cur = p
+        self.damp = True
+
+    def advance(self, cur, prev, out, damp: bool) -> None:
+        """One split step out of place (lfm_advance_split_f32)."""
+        ptr = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        args = []
+        for f in range(4):
+            args += [ptr(cur[f]), ptr(prev[f]), ptr(out[f])]
+        _lib.call("lfm_advance_split_f32", int(self.level), *args, self.table.data_ptr(),
+                  ctypes.byref(self.desc), int(damp), self.N, *self.common,
                   float(self.config.epsilon_w), _stream_handle(self.device))
 
 
@@ -126,15 +225,12 @@ class _Plan:
         n = lat.n
         f32 = dict(dtype=torch.float32, device=lat.device)
 
-        def triple():
-            return [torch.empty(n, **f32), torch.empty(n, **f32) if lat.cx else None,
-                    torch.empty(n, **f32)]
-
-        # checkpoint k: the (current, previous) slot triples before step k*every
-        self.snaps = [(triple(), triple()) for _ in range(math.ceil(steps / every))]
+        # checkpoint k: the (current, previous) slot buffers before step k*every
+        self.snaps = [(lat.new_state_buffers(), lat.new_state_buffers())
+                      for _ in range(math.ceil(steps / every))]
         self.meta = [False] * len(self.snaps)  # damp flag of each checkpoint
         # recomputed states 1 .. every of a segment (state 0 is the checkpoint)
-        self.seg = [triple() for _ in range(every)]
+        self.seg = [lat.new_state_buffers() for _ in range(every)]
         self.g = [[None if (not lat.cx and f in (2, 3)) else torch.zeros(n, **f32)
                    for f in range(6)] for _ in range(2)]
         self.fwd_graph = None
@@ -150,8 +246,7 @@ class _Plan:
                 k = t // self.every
                 cur, prev = self.snaps[k]
                 c, p = lat.cur, 1 - lat.cur
-                for dst, src in ((cur, (lat.pr[c], lat.pi[c] if lat.cx else None, lat.chi[c])),
-                                 (prev, (lat.pr[p], lat.pi[p] if lat.cx else None, lat.chi[p]))):
+                for dst, src in ((cur, lat.slots(c)), (prev, lat.slots(p))):
                     for d, x in zip(dst, src):
                         if d is not None:
                             d.copy_(x)
@@ -175,8 +270,8 @@ class _Plan:
                 lat.advance(states[u], p0 if u == 0 else states[u - 1], states[u + 1],
                             self.meta[si] if u == 0 else True)
             for t in range(e0 - 1, s0 - 1, -1):
-                st, nx = states[t - s0], states[t - s0 + 1]
-                lat.adjoint_step(st[0], st[1], st[2], nx[2], self.g[cur], self.g[1 - cur])
+                lat.adjoint_step(states[t - s0], states[t - s0 + 1], self.g[cur],
+                                 self.g[1 - cur])
                 cur = 1 - cur
         return cur
 
@@ -245,14 +340,14 @@ class LeapfrogFunction(torch.autograd.Function):
 _LATTICES: dict = {}
 
 
-def _lattice_for(config, be: B200Backend) -> _Lattice:
+def _lattice_for(config, be: B200Backend, split_chi: bool = False) -> _Lattice:
     c = config
     key = (str(be.device), int(c.grid_size), int(c.field_level), float(c.boundary_fraction),
            float(c.dt), float(c.kappa), float(c.lambda_self), float(c.chi0), float(c.e0_sq),
-           float(c.epsilon_w))
+           float(c.epsilon_w), bool(split_chi))
     lat = _LATTICES.get(key)
     if lat is None:
-        lat = _LATTICES[key] = _Lattice(config, be)
+        lat = _LATTICES[key] = (_SplitLattice if split_chi else _Lattice)(config, be)
         lat.plans = {}
     return lat
 
@@ -266,7 +361,8 @@ def _plan_for(lat: _Lattice, steps: int, every: int) -> _Plan:
     return plan
 
 
-def leapfrog(config, state, steps: int, every: int | None = None, backend="auto"):
+def leapfrog(config, state, steps: int, every: int | None = None, backend="auto",
+             split_chi: bool = False):
     """Differentiable `steps` leapfrog steps of a REAL/COMPLEX state.
 
     state: six tensors (N, N, N) float32 on the device in the reference
@@ -275,9 +371,14 @@ def leapfrog(config, state, steps: int, every: int | None = None, backend="auto"
     (default ceil(sqrt(steps))).  Buffers and CUDA graphs are cached per
     lattice and schedule, so repeated calls (an optimisation loop) replay
     one graph for the forward and one for the backward.
+
+    split_chi: step with chi held as chi0 + hi + lo (the split-chi step) in
+    the forward and in the recomputed segments; chi and chi_prev may then be
+    given in float64 and come back in float64, so a loss on chi keeps about
+    48 bits.  The adjoint step is the same float32 one.
     """
     be = backend if isinstance(backend, B200Backend) else get_backend(backend)
-    lat = _lattice_for(config, be)
+    lat = _lattice_for(config, be, split_chi)
     steps = int(steps)
     if steps < 1:
         raise ValueError("steps must be >= 1")
@@ -295,14 +396,16 @@ def leapfrog(config, state, steps: int, every: int | None = None, backend="auto"
     return LeapfrogFunction.apply(_plan_for(lat, steps, every), *state)
 
 
-def memory_bytes(config, steps: int, every: int | None = None) -> dict:
-    """Device bytes the checkpoints and the segment buffer of leapfrog() take."""
+def memory_bytes(config, steps: int, every: int | None = None, split_chi: bool = False) -> dict:
+    """Device bytes the checkpoints and the segment buffer of leapfrog() take (split_chi:
+    chi's lo slots besides)."""
     n = int(config.grid_size) ** 3
     cx = int(config.field_level) == FieldLevel.COMPLEX
     every = int(every or math.ceil(math.sqrt(steps)))
     snaps = math.ceil(steps / every)
-    per_snap = (6 if cx else 4) * 4 * n
-    seg = every * (3 if cx else 2) * 4 * n
+    extra = 1 if split_chi else 0
+    per_snap = 2 * ((3 if cx else 2) + extra) * 4 * n
+    seg = every * ((3 if cx else 2) + extra) * 4 * n
     return {"checkpoints": snaps, "checkpoint_bytes": snaps * per_snap, "segment_bytes": seg,
             "all_states_bytes": steps * (3 if cx else 2) * 4 * n}
 

@@ -155,7 +155,7 @@ def test_one_adjoint_step_is_the_float64_vjp(be, level):
     chi_next = f32(out[4].detach())
     g_out = [f32(c) for c in cot]
     g_in = [None if c is None else torch.empty_like(c) for c in g_out]
-    lat.adjoint_step(f32(st[0]), f32(st[2]), f32(st[4]), chi_next, g_out, g_in)
+    lat.adjoint_step([f32(st[0]), f32(st[2]), f32(st[4])], [None, None, chi_next], g_out, g_in)
     torch.cuda.synchronize()
     for f, (got, w) in enumerate(zip(g_in, want)):
         if w is None:

@@ -65,6 +65,9 @@ TOL = {
     # the per-cell chi offset's difference quotient carries the O(h^2) truncation
     # (measured 1.6e-3 with the standing packets)
     "c5_autograd_vs_fd": 1e-4, "c5_autograd_vs_fd_dchi": 5e-3,
+    # config 5 with the split-chi forward: the workload's own loss against float64
+    # central differences (h = 1e-3), amplitude, centre and phase
+    "c5_split_vs_fd": 1e-4,
 }
 
 
@@ -355,6 +358,20 @@ def test_config5_adjoint_complex96_500_steps(be):
     cot32 = 2.0 * (chi32.detach().double() - target)
     _, g_floor, _ = f64_grads(cot32)
 
+    # (4) the split-chi forward (chi as chi0 + hi + lo, to about 48 bits, returned in
+    # float64): the gradient of the workload's own loss
+    def cuda_run_split():
+        p32 = [p.float().clone().requires_grad_(True) for p in params]
+        d64 = torch.zeros((N, N, N), device=dev, dtype=torch.float64, requires_grad=True)
+        st = soliton_state(N, *p32, sigma, cfg.chi0, None, True, omega_dt=cfg.chi0 * cfg.dt)
+        st[4] = st[5] = cfg.chi0 + d64
+        out = leapfrog(cfg, st, steps, backend=be, split_chi=True)
+        return p32 + [d64], out[4].view(N, N, N)
+
+    inp, chi_sp = cuda_run_split()
+    loss_sp = ((chi_sp - target) ** 2).sum()
+    g_sp = torch.autograd.grad(loss_sp, inp)
+
     # (2) float64 central differences, h = 1e-3
     h = 1e-3
     probes = [(0, (0,)), (0, (1,)), (1, (0, 0)), (1, (0, 1)), (1, (1, 2)), (2, (0,)), (2, (1,))]
@@ -408,6 +425,9 @@ def test_config5_adjoint_complex96_500_steps(be):
         "f32_loss_gradient_vs_f64": {n: rel(a, b) for n, a, b in zip(names, g32, g64)},
         "float32_forward_floor": {n: rel(a, b) for n, a, b in zip(names, g_floor, g64)},
         "f32_loss_gradient_vs_fd": rel_fd(g32),
+        "chi_split_max_abs_error": float((chi_sp.detach() - chi64).abs().max()),
+        "split_loss_gradient_vs_f64": {n: rel(a, b) for n, a, b in zip(names, g_sp, g64)},
+        "split_loss_gradient_vs_fd": rel_fd(g_sp),
         "fd_h": h, "fd_probes": len(fd),
     }
     record("config5_adjoint_complex96_500", res)
@@ -430,6 +450,9 @@ def test_config5_adjoint_complex96_500_steps(be):
     for n in names:
         assert res["f32_loss_gradient_vs_f64"][n] <= 1.5 * res["float32_forward_floor"][n] + 1e-3
     assert math.isfinite(res["loss_f32"]) and res["loss_f64"] > 0.0
+    # (4) with the split-chi forward the workload's own loss is resolved
+    sp = res["split_loss_gradient_vs_fd"]
+    assert max(sp[n] for n in ("amplitude", "centre", "phase")) < TOL["c5_split_vs_fd"]
 
 
 if __name__ == "__main__":
