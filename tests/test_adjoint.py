@@ -68,6 +68,22 @@ def linear_target(N, device, seed=12):
     return (w, v)
 
 
+# ---------------------------------------------------------------- host only
+def test_checkpoint_memory_of_both_forms():
+    from lfm_b200.adjoint import memory_bytes
+    from lfm_b200.config import gravity_em
+
+    cfg = gravity_em(96)
+    n = 96**3
+    plain, split = memory_bytes(cfg, 500), memory_bytes(cfg, 500, split_chi=True)
+    # every = ceil(sqrt(500)) = 23 steps, 22 checkpoints
+    assert plain["checkpoints"] == split["checkpoints"] == 22
+    assert plain["checkpoint_bytes"] == 22 * 6 * 4 * n
+    assert split["checkpoint_bytes"] == 22 * 8 * 4 * n
+    assert plain["segment_bytes"] == 23 * 3 * 4 * n
+    assert split["segment_bytes"] == 23 * 4 * 4 * n
+
+
 # ---------------------------------------------------------------- oracle pin (CPU)
 @pytest.mark.parametrize("level", ["real", "complex"])
 def test_float64_autograd_matches_central_differences(level):
@@ -268,6 +284,73 @@ def test_target_distance_loss_of_the_adjoint_workload(be):
     print("seeded float64 VJP:", errs, "| all-float64 loss:", errs_full,
           "| loss", loss.item(), "vs", full.item())
     assert max(errs.values()) < GRAD_RTOL, errs
+
+
+@pytest.mark.gpu
+def test_split_chi_forward_resolves_the_target_distance_loss(be):
+    """The same loss with leapfrog(split_chi=True): chi runs as chi0 + hi + lo (about 48
+    bits) and comes back in float64, so the gradient of the float32-state run's own loss
+    matches the gradient of the all-float64 loss (which the float32 forward cannot)."""
+    from lfm_b200.adjoint import leapfrog, soliton_state
+
+    N, steps, sigma = 20, 40, 2.0
+    cfg = config5_like(N, True)
+    dev = be.device
+    params = make_params(2, N, 6, dev, torch.float64)
+    amp, cen, ph, _ = params
+    from lfm_b200.mask import boundary_mask
+
+    # the target: the float64 transcription from perturbed packet parameters
+    with torch.no_grad():
+        st_t = soliton_state(N, 1.2 * amp, cen + 1.5, ph + 0.7, sigma, cfg.chi0,
+                             torch.zeros(N, N, N, device=dev, dtype=torch.float64), True,
+                             device=dev, dtype=torch.float64)
+        mask = torch.from_numpy(boundary_mask(N, cfg.boundary_fraction).reshape(N, N, N)).to(
+            dev, torch.float64)
+        s = {"pr": st_t[0], "prp": st_t[1], "pi": st_t[2], "pip": st_t[3], "chi": st_t[4],
+             "chip": st_t[5]}
+        target = TR.run(cfg, s, steps, mask)["chi"].reshape(N, N, N)
+
+    p32 = [p.detach().to(torch.float32).clone().requires_grad_(True) for p in params[:3]]
+    d64 = params[3].detach().clone().requires_grad_(True)
+    st = soliton_state(N, *p32, sigma, cfg.chi0, None, True)
+    st[4] = st[5] = cfg.chi0 + d64
+    out = leapfrog(cfg, st, steps, backend=be, split_chi=True)
+    assert out[4].dtype == torch.float64
+    loss = ((out[4] - target) ** 2).sum()
+    grads = torch.autograd.grad(loss, p32 + [d64])
+
+    # the all-float64 loss from the same (float32-rounded) packet parameters
+    fp = [p.detach().double().clone().requires_grad_(True) for p in p32] + [
+        params[3].clone().requires_grad_(True)]
+    full = ref_loss(cfg, fp, target, steps, sigma, True)
+    want = torch.autograd.grad(full, fp)
+    names = ("amplitude", "centre", "phase", "dchi")
+    errs = {n: rel(g, w) for n, g, w in zip(names, grads, want)}
+    print("split chi, all-float64 loss:", errs, "| loss", loss.item(), "vs", full.item())
+    assert max(errs.values()) < GRAD_RTOL, errs
+
+
+@pytest.mark.gpu
+def test_split_chi_checkpoint_interval_does_not_change_gradients(be):
+    from lfm_b200.adjoint import leapfrog, soliton_state
+
+    N, steps, sigma = 16, 24, 2.0
+    cfg = config5_like(N, True)
+    params = make_params(2, N, 7, be.device, torch.float64)
+    runs = []
+    for every in (1, 5, 24):
+        p32 = [p.detach().float().clone().requires_grad_(True) for p in params[:3]]
+        d64 = params[3].detach().clone().requires_grad_(True)
+        st = soliton_state(N, *p32, sigma, cfg.chi0, None, True)
+        st[4] = st[5] = cfg.chi0 + d64
+        out = leapfrog(cfg, st, steps, every=every, backend=be, split_chi=True)
+        loss = ((out[4] - cfg.chi0) ** 2).sum()
+        runs.append((loss.item(), torch.autograd.grad(loss, p32 + [d64])))
+    for loss, grads in runs[1:]:
+        assert loss == runs[0][0]
+        for g, g0 in zip(grads, runs[0][1]):
+            assert torch.equal(g, g0)
 
 
 @pytest.mark.gpu
