@@ -1320,6 +1320,7 @@ __device__ __forceinline__ void batch_run_class(const BatchParams& B, float* sme
                                                 int& s_item) {
   constexpr BatchShape K = kBatchShapes[C];
   constexpr int V = K.level == LFM_REAL ? 4 : 2;
+  // (the GeomBT arguments of a run-time class are placeholders: that branch is not taken)
   using G = std::conditional_t<K.N == 0, GeomRTT<TABM>,
                                GeomBT<(K.N ? K.N : 4), (K.TJ ? K.TJ : 1),
                                       QFields<K.level>::ns, TABM>>;
@@ -1335,7 +1336,9 @@ __device__ __forceinline__ void batch_run_class(const BatchParams& B, float* sme
 // the next at once, so the launch has a single tail (the smallest COMPLEX
 // items).  The class loops run one after the other, so their register
 // demands do not add up.  TABM: the sponge tables in shared memory
-// (1, B.tab_off >= 0) or through L1 (-1).
+// (1, B.tab_off >= 0) or through L1 (-1).  The explicit one block per SM in
+// the launch bounds keeps ptxas at 128 registers: without it, for a kernel
+// this size, it allocated 64 and spilled kilobytes per thread.
 template <int TABM>
 __global__ void __launch_bounds__(512, 1) tma_batch_kernel(const __grid_constant__ BatchParams B) {
   extern __shared__ __align__(128) float smem[];
