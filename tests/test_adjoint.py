@@ -332,17 +332,19 @@ def test_split_chi_forward_resolves_the_target_distance_loss(be):
 
 
 @pytest.mark.gpu
-def test_split_chi_checkpoint_interval_does_not_change_gradients(be):
+@pytest.mark.parametrize("level", ["real", "complex"])
+def test_split_chi_checkpoint_interval_does_not_change_gradients(be, level):
     from lfm_b200.adjoint import leapfrog, soliton_state
 
     N, steps, sigma = 16, 24, 2.0
-    cfg = config5_like(N, True)
+    cx = level == "complex"
+    cfg = config5_like(N, cx)
     params = make_params(2, N, 7, be.device, torch.float64)
     runs = []
     for every in (1, 5, 24):
         p32 = [p.detach().float().clone().requires_grad_(True) for p in params[:3]]
         d64 = params[3].detach().clone().requires_grad_(True)
-        st = soliton_state(N, *p32, sigma, cfg.chi0, None, True)
+        st = soliton_state(N, *p32, sigma, cfg.chi0, None, cx)
         st[4] = st[5] = cfg.chi0 + d64
         out = leapfrog(cfg, st, steps, every=every, backend=be, split_chi=True)
         loss = ((out[4] - cfg.chi0) ** 2).sum()
@@ -365,6 +367,33 @@ def test_checkpoint_interval_does_not_change_gradients(be):
         assert loss == runs[0][0]
         for g, g0 in zip(grads, runs[0][1]):
             assert torch.equal(g, g0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", ["real", "complex"])
+def test_split_chi_forward_matches_split_evolver(be, level):
+    """leapfrog(split_chi=True) steps as SplitChiEvolver does: the same bits of Psi and of
+    chi's float64 value."""
+    from lfm_b200.adjoint import leapfrog, soliton_state
+    from lfm_b200.split import SplitChiEvolver
+
+    N, steps = 16, 13
+    cx = level == "complex"
+    cfg = config5_like(N, cx)
+    params = make_params(2, N, 8, be.device, torch.float64)
+    st = soliton_state(N, *[p.float() for p in params[:3]], 2.0, cfg.chi0, None, cx)
+    st[4] = st[5] = cfg.chi0 + params[3]
+    out = leapfrog(cfg, st, steps, backend=be, split_chi=True)
+    ev = SplitChiEvolver(cfg, backend=be)
+    ev.set_psi_real(st[0])
+    if cx:
+        ev.set_psi_imag(st[2])
+    ev.set_chi(st[4])
+    ev.evolve(steps)
+    assert torch.equal(out[0].cpu(), torch.from_numpy(ev.get_psi_real()))
+    if cx:
+        assert torch.equal(out[2].cpu(), torch.from_numpy(ev.get_psi_imag()))
+    assert torch.equal(out[4].reshape(-1).cpu(), ev.chi64().cpu())
 
 
 @pytest.mark.gpu
